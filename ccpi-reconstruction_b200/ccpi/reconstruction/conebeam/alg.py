@@ -1,0 +1,172 @@
+"""``ccpi.reconstruction.conebeam.alg`` on a B200.
+
+Same functions, argument order and conventions as the reference module
+(Wrappers/Python/src/conebeam_module.cpp:32-41, conebeam_wrapper.cpp):
+
+* ``pixels``: (n_angles, n_h, n_v) projections (no transpose, unlike the
+  parallel-beam module); transmission unless ``is_pixels_in_log``;
+* ``angles`` in degrees; the source sits at (-source_to_sample, 0, 0) and
+  the detector plane at source_to_detector - source_to_sample;
+* ``pixels_per_voxel``, ``pixel_h_size``, ``pixel_v_size`` and
+  ``mask_radius`` set the voxel grid the reference derives
+  (Readers/xtek.cpp:760-798); the centre of rotation is searched on the
+  data (xtek.cpp:671-758) before solving;
+* ``h_offsets``, ``v_offsets``, ``beam_harden``, ``full_vox_origin`` and
+  ``voxel_size`` are accepted and, as in the reference, do not change the
+  result (the reference copies the last two into locals it overwrites);
+* result: a new float32 volume (nx, ny, nz), clamped at zero.
+
+``create_sinogram`` is the cone forward projection of an explicit geometry
+(angles in radians there, as in the reference).  Deviations as in the
+parallel-beam module: conversion instead of reinterpretation of other
+dtypes, exceptions instead of (1, 1, 1) zero arrays, ``nthreads`` ignored.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .. import _native as N
+
+__all__ = ["cgls", "cgls_conv", "sirt", "mlem", "cgls_tikhonov", "cgls_TVreg",
+           "create_sinogram", "grid", "find_centre"]
+
+
+def grid(n_angles, n_h, n_v, pixels_per_voxel, source_to_sample, source_to_detector,
+         pixel_h_size, pixel_v_size, mask_radius):
+    """((nx, ny, nz, n_v_padded, v_offset), (voxel xy, voxel z, origin x, y, z))."""
+    dims = np.zeros(5, np.int32)
+    geom = np.zeros(5, np.float64)
+    N.check(N.lib.ccpi_cb_grid(int(n_angles), int(n_h), int(n_v), int(pixels_per_voxel),
+                               float(source_to_sample), float(source_to_detector),
+                               float(pixel_h_size), float(pixel_v_size), float(mask_radius),
+                               dims, geom), "conebeam grid")
+    return tuple(int(d) for d in dims), tuple(float(g) for g in geom)
+
+
+def find_centre(padded_log_sino, angles, source_to_sample, source_to_detector, pixel_h_size):
+    """Source y offset of the reference's centre search on a padded log
+    sinogram (n_angles, n_h, n_v_padded)."""
+    s = N.f32(padded_log_sino, "sinogram", 3)
+    a = N.f32(angles, "angles", 1)
+    y = ctypes.c_double(0.0)
+    N.check(N.lib.ccpi_cb_find_centre(s, *s.shape, a, float(source_to_sample),
+                                      float(source_to_detector), float(pixel_h_size),
+                                      ctypes.byref(y)), "conebeam find_centre")
+    return y.value
+
+
+def _reconstruct(alg, pixels, angles, pixels_per_voxel, source_to_sample, source_to_detector,
+                 pixel_h_size, pixel_v_size, mask_radius, niterations, nthreads,
+                 is_pixels_in_log, regularize=0.0, norm_r=None, real_norms=False):
+    pix = N.f32(pixels, "pixels", 3)
+    ang = N.f32(angles, "angles", 1)
+    na, nh, nv = pix.shape
+    if ang.shape[0] != na:
+        raise ValueError(f"Number of projections ({na}) doesn't match angle array "
+                         f"({ang.shape[0]})")
+    niterations = int(niterations)
+    if niterations < 0:
+        raise ValueError("niterations must be >= 0")
+    dims, _ = grid(na, nh, nv, pixels_per_voxel, source_to_sample, source_to_detector,
+                   pixel_h_size, pixel_v_size, mask_radius)
+    out = np.zeros(dims[:3], np.float32)
+    norms = np.zeros(max(niterations, 1), np.float64)
+    N.check(N.lib.ccpi_cb_reconstruct(alg, pix, na, nh, nv, ang, int(pixels_per_voxel),
+                                      float(source_to_sample), float(source_to_detector),
+                                      float(pixel_h_size), float(pixel_v_size),
+                                      float(mask_radius), niterations, int(nthreads),
+                                      int(bool(is_pixels_in_log)), float(regularize),
+                                      norms.ctypes.data, out), "conebeam reconstruction")
+    if norm_r is not None:
+        nr = np.asarray(norm_r)
+        n = min(niterations, nr.shape[0]) if nr.ndim == 1 else 0
+        if real_norms:
+            nr[:n] = norms[:n]
+        elif n:
+            # conebeam_wrapper.cpp:84-93 overwrites norm_r with zeros
+            nr[:n] = 0
+    return out
+
+
+def cgls(pixels, angles, h_offsets, v_offsets, pixels_per_voxel, source_to_sample,
+         source_to_detector, pixel_h_size, pixel_v_size, mask_radius, beam_harden,
+         full_vox_origin, voxel_size, niterations, nthreads, is_pixels_in_log=True):
+    return _reconstruct(N.CGLS, pixels, angles, pixels_per_voxel, source_to_sample,
+                        source_to_detector, pixel_h_size, pixel_v_size, mask_radius,
+                        niterations, nthreads, is_pixels_in_log)
+
+
+def sirt(pixels, angles, h_offsets, v_offsets, pixels_per_voxel, source_to_sample,
+         source_to_detector, pixel_h_size, pixel_v_size, mask_radius, beam_harden,
+         full_vox_origin, voxel_size, niterations, nthreads, is_pixels_in_log=True):
+    return _reconstruct(N.SIRT, pixels, angles, pixels_per_voxel, source_to_sample,
+                        source_to_detector, pixel_h_size, pixel_v_size, mask_radius,
+                        niterations, nthreads, is_pixels_in_log)
+
+
+def mlem(pixels, angles, h_offsets, v_offsets, pixels_per_voxel, source_to_sample,
+         source_to_detector, pixel_h_size, pixel_v_size, mask_radius, beam_harden,
+         full_vox_origin, voxel_size, niterations, nthreads, is_pixels_in_log=True):
+    return _reconstruct(N.MLEM, pixels, angles, pixels_per_voxel, source_to_sample,
+                        source_to_detector, pixel_h_size, pixel_v_size, mask_radius,
+                        niterations, nthreads, is_pixels_in_log)
+
+
+def cgls_conv(pixels, angles, h_offsets, v_offsets, pixels_per_voxel, source_to_sample,
+              source_to_detector, pixel_h_size, pixel_v_size, mask_radius, beam_harden,
+              full_vox_origin, voxel_size, niterations, nthreads, norm_r,
+              is_pixels_in_log=True, real_norms=False):
+    return _reconstruct(N.CGLS, pixels, angles, pixels_per_voxel, source_to_sample,
+                        source_to_detector, pixel_h_size, pixel_v_size, mask_radius,
+                        niterations, nthreads, is_pixels_in_log, norm_r=norm_r,
+                        real_norms=real_norms)
+
+
+def cgls_tikhonov(pixels, angles, h_offsets, v_offsets, pixels_per_voxel, source_to_sample,
+                  source_to_detector, pixel_h_size, pixel_v_size, mask_radius, beam_harden,
+                  full_vox_origin, voxel_size, niterations, nthreads, regularize, norm_r,
+                  is_pixels_in_log=True, real_norms=False):
+    return _reconstruct(N.CGLS_TIKHONOV, pixels, angles, pixels_per_voxel, source_to_sample,
+                        source_to_detector, pixel_h_size, pixel_v_size, mask_radius,
+                        niterations, nthreads, is_pixels_in_log, regularize, norm_r,
+                        real_norms=real_norms)
+
+
+def cgls_TVreg(pixels, angles, h_offsets, v_offsets, pixels_per_voxel, source_to_sample,
+               source_to_detector, pixel_h_size, pixel_v_size, mask_radius, beam_harden,
+               full_vox_origin, voxel_size, niterations, nthreads, regularize, norm_r,
+               is_pixels_in_log=True, real_norms=False):
+    return _reconstruct(N.CGLS_TV, pixels, angles, pixels_per_voxel, source_to_sample,
+                        source_to_detector, pixel_h_size, pixel_v_size, mask_radius,
+                        niterations, nthreads, is_pixels_in_log, regularize, norm_r,
+                        real_norms=real_norms)
+
+
+def create_sinogram(source_x, source_y, source_z, detector_x, h_pixels, v_pixels, angles,
+                    voxels, grid_offset, voxel_size):
+    """Cone forward projection with explicit geometry
+    (conebeam_wrapper.cpp:346-400): angles in radians, output
+    (n_angles, n_h, n_v)."""
+    vol = N.f32(voxels, "voxels", 3)
+    # the reference reads every geometry value through float32
+    h = np.asarray(h_pixels, np.float32).astype(np.float64)
+    v = np.asarray(v_pixels, np.float32).astype(np.float64)
+    a = np.asarray(angles, np.float32).astype(np.float64)
+    g = N.Geometry()
+    g.kind = N.CONE
+    keep = [np.ascontiguousarray(x) for x in (a, h, v)]
+    g.angles, g.h_pixels, g.v_pixels = (x.ctypes.data for x in keep)
+    g.n_angles, g.n_h, g.n_v = len(a), len(h), len(v)
+    f = lambda x: float(np.float32(x))  # noqa: E731
+    g.source = (ctypes.c_double * 3)(f(source_x), f(source_y), f(source_z))
+    g.detector_x = f(detector_x)
+    go = np.asarray(grid_offset, np.float32)
+    vs = np.asarray(voxel_size, np.float32)
+    g.origin = (ctypes.c_double * 3)(*(float(x) for x in go[:3]))
+    g.voxel_size = (ctypes.c_double * 3)(*(float(x) for x in vs[:3]))
+    g.nx, g.ny, g.nz = vol.shape
+    out = np.zeros((len(a), len(h), len(v)), np.float32)
+    N.check(N.lib.ccpi_cb_create_sinogram(ctypes.byref(g), vol, out), "create_sinogram")
+    return out

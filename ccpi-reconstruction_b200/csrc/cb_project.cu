@@ -1,0 +1,589 @@
+// Cone-beam projectors for sm_100a.
+//
+// Forward (cone_beam::f2D, Core/src/c2D.cpp:469-625): ray-driven.  One warp
+// owns one ray (angle a, detector column h).  The warp walks the ray's xy
+// Siddon path once in voxel-normalised coordinates (c2D.cpp:193-467, FP64
+// geometry, alphas rounded to float exactly as the reference stores them)
+// and stages the (alpha, column) list in its own slice of shared memory.
+// The lanes then own detector rows v and replay the list: each xy segment is
+// split across at most two z slices with the reference's float arithmetic
+// and its three row regimes (all-inside, lower edge, upper edge;
+// c2D.cpp:17-191), and the row is finally scaled by the source-pixel
+// distance.  Per row the additions happen in the reference's order with
+// unfused float operations, so the result matches the reference bit for bit.
+//
+// Backward (cone_beam::b2D, c2D.cpp:948-1119): voxel-column gather, the
+// reference's design.  One CTA owns one xy column; it finds, angle chunk by
+// angle chunk, every (angle, detector column) ray that crosses the column
+// with the reference's entry/exit alphas (c2D.cpp:788-946), then its warps
+// spread each ray's detector rows over the column's z slices (c2D.cpp:
+// 640-751) into a shared-memory accumulator.  Shared-memory float atomics
+// make the summation order unspecified, so this projector agrees with the
+// reference to float rounding rather than bit for bit.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ccpi {
+namespace {
+
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float fmin_ref(float a, float b) { return (b < a) ? b : a; }
+
+// xy walk of ray p1 -> p2 over the whole volume; writes alphas[0..n-1] and
+// cells[0..n-2] (x*ny + y, or -1) with lane 0; returns n (0 if missed).
+__device__ int cb_walk(const Geom &g, double p1x, double p1y, double p2x, double p2y,
+                       float *alphas, int *cells, int cap) {
+  const double eps = double(kEps);
+  const int nx = g.nx, ny = g.ny;
+  const bool w = (threadIdx.x & 31) == 0;
+  const double q1x = (p1x - g.origin[0]) / g.size[0];
+  const double q1y = (p1y - g.origin[1]) / g.size[1];
+  const double q2x = (p2x - g.origin[0]) / g.size[0];
+  const double q2y = (p2y - g.origin[1]) / g.size[1];
+  const double ddx = q2x - q1x, ddy = q2y - q1y;
+  const double idx = 1.0 / ddx, idy = 1.0 / ddy;
+  int n = 0;
+  if (fabs(ddx) < eps) {
+    if (fabs(ddy) < eps)
+      return 0;
+    const int i = int(floor(q1x));
+    if (i < 0 || i >= nx)
+      return 0;
+    if (ddy < 0.0) {
+      if (w)
+        alphas[0] = float((double(ny) - q1y) * idy);
+      for (int j = ny - 1; j >= 0; j--) {
+        if (w) {
+          alphas[ny - j] = float((double(j) - q1y) * idy);
+          cells[ny - 1 - j] = i * ny + j;
+        }
+      }
+    } else {
+      if (w)
+        alphas[0] = float((0.0 - q1y) * idy);
+      for (int j = 0; j < ny; j++) {
+        if (w) {
+          alphas[j + 1] = float((double(j + 1) - q1y) * idy);
+          cells[j] = i * ny + j;
+        }
+      }
+    }
+    return ny + 1;
+  }
+  if (fabs(ddy) < eps) {
+    const int j = int(floor(q1y));
+    if (j < 0 || j >= ny)
+      return 0;
+    if (ddx < 0.0) {
+      if (w)
+        alphas[0] = float((double(nx) - q1x) * idx);
+      for (int i = nx - 1; i >= 0; i--) {
+        if (w) {
+          alphas[nx - i] = float((double(i) - q1x) * idx);
+          cells[nx - 1 - i] = i * ny + j;
+        }
+      }
+    } else {
+      if (w)
+        alphas[0] = float((0.0 - q1x) * idx);
+      for (int i = 0; i < nx; i++) {
+        if (w) {
+          alphas[i + 1] = float((double(i + 1) - q1x) * idx);
+          cells[i] = i * ny + j;
+        }
+      }
+    }
+    return nx + 1;
+  }
+  const double ax0 = (0.0 - q1x) * idx, ay0 = (0.0 - q1y) * idy;
+  const double axn = (double(nx) - q1x) * idx, ayn = (double(ny) - q1y) * idy;
+  const double amin = dmax(dmax(dmin(ax0, axn), dmin(ay0, ayn)), 0.0);
+  const double amax = dmin(dmin(dmax(ax0, axn), dmax(ay0, ayn)), 1.0);
+  if (!(amin < amax - eps))
+    return 0;
+  const int sx = ddx > 0.0 ? 1 : -1, sy = ddy > 0.0 ? 1 : -1;
+  int x = 0, y = 0;
+  const bool x_face_first = !(sx > 0 && sy < 0);
+  const double axe = sx > 0 ? ax0 : axn, aye = sy > 0 ? ay0 : ayn;
+  auto cx = [&]() { return int(floor(q1x + amin * ddx)); };
+  auto cy = [&]() { return int(floor(q1y + amin * ddy)); };
+  if (x_face_first) {
+    if (amin == axe) {
+      x = sx > 0 ? 0 : nx - 1;
+      y = (sx < 0 && sy < 0 && amin == ayn) ? ny - 1 : cy();
+    } else if (amin == aye) {
+      x = cx();
+      y = sy > 0 ? 0 : ny - 1;
+    }
+  } else {
+    if (amin == aye) {
+      x = cx();
+      y = ny - 1;
+    } else if (amin == axe) {
+      x = 0;
+      y = cy();
+    }
+  }
+  if (w)
+    alphas[0] = float(amin);
+  n = 1;
+  while ((sx > 0 ? x < nx : x >= 0) && (sy > 0 ? y < ny : y >= 0) && n < cap) {
+    const double nxa = (double(sx > 0 ? x + 1 : x) - q1x) * idx;
+    const double nya = (double(sy > 0 ? y + 1 : y) - q1y) * idy;
+    const int cell = (x >= 0 && x < nx && y >= 0 && y < ny) ? x * ny + y : -1;
+    double an;
+    if (nxa < nya - eps) {
+      an = nxa;
+      x += sx;
+    } else if (nya < nxa - eps) {
+      an = nya;
+      y += sy;
+    } else {
+      an = dmax(nxa, nya);
+      x += sx;
+      y += sy;
+    }
+    if (w) {
+      cells[n - 1] = cell;
+      alphas[n] = float(an);
+    }
+    n++;
+  }
+  return n;
+}
+
+template <int EPI>
+__device__ __forceinline__ float cb_fp_epi(float acc, i64 idx, const Epi &e, double &ssq) {
+  if (EPI == EPI_NORM) {
+    ssq += double(acc) * double(acc);
+    return acc;
+  } else if (EPI == EPI_SIRT) {
+    return __fmul_rn(__fadd_rn(-acc, e.b[idx]), e.w[idx]);
+  } else if (EPI == EPI_MLEM) {
+    const float q = (acc != 0.0f) ? __fdiv_rn(e.b[idx], acc) : 0.0f;
+    return (q < 0.0f) ? 0.0f : q;
+  }
+  return acc;
+}
+
+constexpr int kFpWarps = 4;
+constexpr int kRowsPerLane = 8;
+
+template <int EPI>
+__global__ void __launch_bounds__(kFpWarps * 32)
+    cb_fp_kernel(Geom g, const float *__restrict__ vol, float *__restrict__ pix, Epi e,
+                 const int2 *__restrict__ hrange, int cap) {
+  extern __shared__ unsigned char smem_raw[];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float *alphas = reinterpret_cast<float *>(smem_raw) + size_t(wib) * 2 * cap;
+  int *cells = reinterpret_cast<int *>(alphas + cap);
+  const int nrays = g.na * g.nh;
+  const int nzm1 = g.nz - 1, mid = g.mid;
+  const float pzbz = g.pzbz, pzbz1 = g.pzbz1, inv_dz = g.inv_dz;
+  double ssq = 0.0;
+  for (int ray = blockIdx.x * kFpWarps + wib; ray < nrays; ray += gridDim.x * kFpWarps) {
+    const int a = ray / g.nh, h = ray - a * g.nh;
+    const int2 hr = hrange[a];
+    int n = 0;
+    if (h >= hr.x && h <= hr.y) {
+      const double c = g.cosA[a], s = g.sinA[a];
+      const double p2x = c * g.detx - s * g.hpix[h];
+      const double p2y = s * g.detx + c * g.hpix[h];
+      n = cb_walk(g, g.p1x[a], g.p1y[a], p2x, p2y, alphas, cells, cap);
+    }
+    __syncwarp();
+    // Row regimes (c2D.cpp:45-99), evaluated warp-parallel.
+    int ncom = 0, min_v_all = mid, max_v_all = mid - 1;
+    if (n >= 2) {
+      int min_xy_all = n, max_xy_all = n;
+      const float dz0 = g.dz[0], dzl = g.dz[g.nv - 1];
+      bool got_lo = false, got_hi = false;
+      for (int m0 = 1; m0 < n && !(got_lo && got_hi); m0 += 32) {
+        const int m = m0 + lane;
+        int klo = 1, khi = nzm1 - 1;
+        if (m < n) {
+          const float av = __fmul_rn(alphas[m - 1], inv_dz);
+          klo = int(floorf(__fadd_rn(pzbz, __fmul_rn(av, dz0))));
+          khi = int(floorf(__fadd_rn(pzbz, __fmul_rn(av, dzl))));
+        }
+        if (!got_lo) {
+          const unsigned b = __ballot_sync(0xffffffffu, m < n && klo <= 0);
+          if (b) {
+            const int src = __ffs(b) - 1;
+            const int k = __shfl_sync(0xffffffffu, klo, src);
+            min_xy_all = (k == 0) ? m0 + src : 0;
+            got_lo = true;
+          }
+        }
+        if (!got_hi) {
+          const unsigned b = __ballot_sync(0xffffffffu, m < n && khi >= nzm1);
+          if (b) {
+            const int src = __ffs(b) - 1;
+            const int k = __shfl_sync(0xffffffffu, khi, src);
+            max_xy_all = (k == nzm1) ? m0 + src : 0;
+            got_hi = true;
+          }
+        }
+      }
+      ncom = min(min_xy_all, max_xy_all);
+      const float avl = __fmul_rn(alphas[n - 2], inv_dz);
+      for (int v0 = 0; v0 < mid; v0 += 32) {
+        const int v = v0 + lane;
+        const bool ok = v < mid && int(floorf(__fadd_rn(pzbz, __fmul_rn(avl, g.dz[v])))) > 0;
+        const unsigned b = __ballot_sync(0xffffffffu, ok);
+        if (b) {
+          min_v_all = v0 + __ffs(b) - 1;
+          break;
+        }
+      }
+      for (int v1 = g.nv - 1; v1 >= mid; v1 -= 32) {
+        const int v = v1 - lane;
+        const bool ok =
+            v >= mid && int(floorf(__fadd_rn(pzbz, __fmul_rn(avl, g.dz[v])))) < nzm1;
+        const unsigned b = __ballot_sync(0xffffffffu, ok);
+        if (b) {
+          max_v_all = v1 - (__ffs(b) - 1);
+          break;
+        }
+      }
+    }
+    // Rows, kRowsPerLane per lane per pass.
+    for (int vb = 0; vb < g.nv; vb += 32 * kRowsPerLane) {
+      float acc[kRowsPerLane], dzv[kRowsPerLane], izv[kRowsPerLane];
+#pragma unroll
+      for (int q = 0; q < kRowsPerLane; q++) {
+        const int v = vb + q * 32 + lane;
+        acc[q] = 0.0f;
+        dzv[q] = v < g.nv ? g.dz[v] : 0.0f;
+        izv[q] = v < g.nv ? g.iz[v] : 0.0f;
+      }
+      for (int m = 1; m < n; m++) {
+        const float a0 = alphas[m - 1], a1 = alphas[m];
+        const int cell = cells[m - 1];
+        if (cell < 0)
+          continue;
+        const float *col = vol + i64(cell) * g.nz;
+        const float av = __fmul_rn(a0, inv_dz);
+        const bool all_rows = m < ncom;
+#pragma unroll
+        for (int q = 0; q < kRowsPerLane; q++) {
+          const int v = vb + q * 32 + lane;
+          if (v >= g.nv)
+            continue;
+          const bool inside = all_rows || (v >= min_v_all && v <= max_v_all);
+          if (inside) {
+            const int k = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[q])));
+            const bool below = v < mid;
+            const int kn = below ? k - 1 : k + 1;
+            if (k < 0 || k > nzm1 || kn < 0 || kn > nzm1)
+              continue;
+            const float az = __fmul_rn(g.vz[below ? k : k + 1], izv[q]);
+            const float mz = fmin_ref(az, a1);
+            acc[q] = __fadd_rn(acc[q], __fadd_rn(__fmul_rn(__ldg(col + k), __fsub_rn(mz, a0)),
+                                                 __fmul_rn(__ldg(col + kn), __fsub_rn(a1, mz))));
+          } else if (ncom >= 1) {
+            if (v < min_v_all) {
+              const int k = int(__fadd_rn(pzbz1, __fmul_rn(av, dzv[q]))) - 1;
+              if (k > 0 && k <= nzm1) {
+                const float mz = fmin_ref(__fmul_rn(g.vz[k], izv[q]), a1);
+                acc[q] = __fadd_rn(acc[q],
+                                   __fadd_rn(__fmul_rn(__ldg(col + k), __fsub_rn(mz, a0)),
+                                             __fmul_rn(__ldg(col + k - 1), __fsub_rn(a1, mz))));
+              } else if (k == 0) {
+                const float mz = fmin_ref(__fmul_rn(g.vz[0], izv[q]), a1);
+                acc[q] = __fadd_rn(acc[q], __fmul_rn(__ldg(col), __fsub_rn(mz, a0)));
+              }
+            } else {
+              const int k = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[q])));
+              if (k < nzm1 && k >= 0) {
+                const float mz = fmin_ref(__fmul_rn(g.vz[k + 1], izv[q]), a1);
+                acc[q] = __fadd_rn(acc[q],
+                                   __fadd_rn(__fmul_rn(__ldg(col + k), __fsub_rn(mz, a0)),
+                                             __fmul_rn(__ldg(col + k + 1), __fsub_rn(a1, mz))));
+              } else if (k == nzm1) {
+                const float mz = fmin_ref(__fmul_rn(g.vz[g.nz], izv[q]), a1);
+                acc[q] = __fadd_rn(acc[q], __fmul_rn(__ldg(col + nzm1), __fsub_rn(mz, a0)));
+              }
+            }
+          }
+        }
+      }
+      const i64 rbase = i64(ray) * g.nv;
+#pragma unroll
+      for (int q = 0; q < kRowsPerLane; q++) {
+        const int v = vb + q * 32 + lane;
+        if (v < g.nv) {
+          const float val = __fmul_rn(acc[q], g.dconv[i64(h) * g.nv + v]);
+          pix[rbase + v] = cb_fp_epi<EPI>(val, rbase + v, e, ssq);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (EPI == EPI_NORM) {
+    __shared__ double red[kFpWarps];
+    const double t = cta_sum<kFpWarps>(ssq, red);
+    if (threadIdx.x == 0)
+      e.partials[blockIdx.x] = t;
+  }
+}
+
+// ---- backward
+constexpr int kBpThreads = 256;
+constexpr int kBpAngleChunk = 64;
+constexpr int kBpMaxRaysPerAngle = 24;
+
+// Rays (angle a, columns h) crossing voxel column [x0,xn) x [y0,yn), with
+// their entry/exit alphas (bproject_ah, c2D.cpp:831-936).  Calls f(h, a0, a1).
+template <class F>
+__device__ void cb_column_rays(const Geom &g, int a, double x0, double xn, double y0,
+                               double yn, F &&f) {
+  const double eps = double(kEps);
+  const double c = g.cosA[a], s = g.sinA[a];
+  const double p1x = g.p1x[a], p1y = g.p1y[a];
+  const double dx0 = x0 - p1x, dy0 = y0 - p1y, dxn = xn - p1x, dyn = yn - p1y;
+  const double cx0 = c * x0 - g.src[0], cxn = c * xn - g.src[0];
+  const double sy0 = s * y0, syn = s * yn;
+  double y00, y01, y10, y11;
+  if (fabs(s) > fabs(c)) {
+    const double il = g.cl / s;
+    y00 = (c - dx0 / (sy0 + cx0)) * il;
+    y01 = (c - dx0 / (syn + cx0)) * il;
+    y10 = (c - dxn / (sy0 + cxn)) * il;
+    y11 = (c - dxn / (syn + cxn)) * il;
+  } else {
+    const double il = g.cl / c;
+    y00 = (-s + dy0 / (cx0 + sy0)) * il;
+    y01 = (-s + dyn / (cx0 + syn)) * il;
+    y10 = (-s + dy0 / (cxn + sy0)) * il;
+    y11 = (-s + dyn / (cxn + syn)) * il;
+  }
+  const int h00 = int(floor(y00 * g.cipix + g.chpix0));
+  const int h01 = int(floor(y01 * g.cipix + g.chpix0));
+  const int h10 = int(floor(y10 * g.cipix + g.chpix0));
+  const int h11 = int(floor(y11 * g.cipix + g.chpix0));
+  const int hmin = max(min(min(h00, h01), min(h10, h11)), 0);
+  const int hmax = min(max(max(h00, h01), max(h10, h11)), g.nh - 1);
+  for (int h = hmin; h <= hmax; h++) {
+    const double p2x = g.cdx[a] - s * g.hpix[h];
+    const double p2y = g.sdx[a] + c * g.hpix[h];
+    const double ddx = p2x - p1x, ddy = p2y - p1y;
+    if (fabs(ddx) < eps || fabs(ddy) < eps)
+      continue; // rejected by the reference ("Ooops", c2D.cpp:909-912)
+    const double idx = 1.0 / ddx, idy = 1.0 / ddy;
+    const double ax0 = dx0 * idx, ay0 = dy0 * idy, axn = dxn * idx, ayn = dyn * idy;
+    const double amin = dmax(dmax(dmin(ax0, axn), dmin(ay0, ayn)), 0.0);
+    const double amax = dmin(dmin(dmax(ax0, axn), dmax(ay0, ayn)), 1.0);
+    if (amin < amax - eps)
+      f(h, float(amin), float(amax));
+  }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kBpThreads)
+    cb_bp_kernel(Geom g, const float *__restrict__ pix, float *__restrict__ vol, Epi e,
+                 int *err) {
+  extern __shared__ unsigned char smem_raw[];
+  float *acc = reinterpret_cast<float *>(smem_raw);
+  const int cap = kBpAngleChunk * kBpMaxRaysPerAngle;
+  int *seg_ah = reinterpret_cast<int *>(acc + g.nz);
+  float *seg_a0 = reinterpret_cast<float *>(seg_ah + cap);
+  float *seg_a1 = seg_a0 + cap;
+  __shared__ int s_count, s_minv, s_maxv, s_ovf;
+  const int col = blockIdx.x;
+  const int i = col / g.ny, j = col - (col / g.ny) * g.ny;
+  const double x0 = g.origin[0] + double(i) * g.size[0];
+  const double xn = g.origin[0] + double(i + 1) * g.size[0];
+  const double y0 = g.origin[1] + double(j) * g.size[1];
+  const double yn = g.origin[1] + double(j + 1) * g.size[1];
+  for (int z = threadIdx.x; z < g.nz; z += blockDim.x)
+    acc[z] = 0.0f;
+  if (threadIdx.x == 0) {
+    s_minv = 0;
+    s_maxv = g.nv;
+    s_ovf = 0;
+  }
+  __syncthreads();
+  // rows [min_v, max_v) stay inside the column for every ray (c2D.cpp:657-676)
+  for (int a = threadIdx.x; a < g.na; a += blockDim.x) {
+    int lo = 0, hi = g.nv;
+    cb_column_rays(g, a, x0, xn, y0, yn, [&](int, float a0, float) {
+      lo = max(lo, int(ceilf(__fadd_rn(g.pzdeps, __fdiv_rn(g.z1, a0)))));
+      hi = min(hi, int(floorf(__fadd_rn(g.pzdv, __fdiv_rn(g.znm, a0)))));
+    });
+    atomicMax(&s_minv, lo);
+    atomicMin(&s_maxv, hi);
+  }
+  __syncthreads();
+  const int min_v = s_minv, max_v = s_maxv;
+  const int nzm1 = g.nz - 1, mid = g.mid;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  for (int ac = 0; ac < g.na; ac += kBpAngleChunk) {
+    if (threadIdx.x == 0)
+      s_count = 0;
+    __syncthreads();
+    for (int a = ac + threadIdx.x; a < min(g.na, ac + kBpAngleChunk); a += blockDim.x) {
+      cb_column_rays(g, a, x0, xn, y0, yn, [&](int h, float a0, float a1) {
+        const int slot = atomicAdd(&s_count, 1);
+        if (slot < cap) {
+          seg_ah[slot] = a * g.nh + h;
+          seg_a0[slot] = a0;
+          seg_a1[slot] = a1;
+        } else {
+          s_ovf = 1;
+        }
+      });
+    }
+    __syncthreads();
+    const int nseg = min(s_count, cap);
+    for (int sgi = wib; sgi < nseg; sgi += kBpThreads / 32) {
+      const int ah = seg_ah[sgi];
+      const int h = ah % g.nh;
+      const float a0 = seg_a0[sgi], a1 = seg_a1[sgi];
+      const float av = __fmul_rn(a0, g.inv_dz);
+      const float *prow = pix + i64(ah) * g.nv;
+      const float *drow = g.dconv + i64(h) * g.nv;
+      for (int v = lane; v < g.nv; v += 32) {
+        const float p = __fmul_rn(__ldg(prow + v), __ldg(drow + v));
+        const float dzv = g.dz[v], izv = g.iz[v];
+        if (v >= min_v && v < max_v) {
+          const int k = int(__fadd_rn(g.pzbz, __fmul_rn(av, dzv)));
+          if (v < mid) {
+            if (k < 1 || k > nzm1)
+              continue;
+            const float mz = fmin_ref(__fmul_rn(g.vz[k], izv), a1);
+            atomicAdd(acc + k, __fmul_rn(p, __fsub_rn(mz, a0)));
+            atomicAdd(acc + k - 1, __fmul_rn(p, __fsub_rn(a1, mz)));
+          } else {
+            if (k < 0 || k >= nzm1)
+              continue;
+            const float mz = fmin_ref(__fmul_rn(g.vz[k + 1], izv), a1);
+            atomicAdd(acc + k, __fmul_rn(p, __fsub_rn(mz, a0)));
+            atomicAdd(acc + k + 1, __fmul_rn(p, __fsub_rn(a1, mz)));
+          }
+        } else if (v < min_v) {
+          const int k = int(__fadd_rn(g.pzbz1, __fmul_rn(av, dzv))) - 1;
+          if (k > 0 && k <= nzm1) {
+            const float mz = fmin_ref(__fmul_rn(g.vz[k], izv), a1);
+            atomicAdd(acc + k, __fmul_rn(p, __fsub_rn(mz, a0)));
+            atomicAdd(acc + k - 1, __fmul_rn(p, __fsub_rn(a1, mz)));
+          } else if (k == 0) {
+            const float mz = fmin_ref(__fmul_rn(g.vz[0], izv), a1);
+            atomicAdd(acc, __fmul_rn(p, __fsub_rn(mz, a0)));
+          }
+        } else {
+          const int k = int(__fadd_rn(g.pzbz, __fmul_rn(av, dzv)));
+          if (k < nzm1 && k >= 0) {
+            const float mz = fmin_ref(__fmul_rn(g.vz[k + 1], izv), a1);
+            atomicAdd(acc + k, __fmul_rn(p, __fsub_rn(mz, a0)));
+            atomicAdd(acc + k + 1, __fmul_rn(p, __fsub_rn(a1, mz)));
+          } else if (k == nzm1) {
+            const float mz = fmin_ref(__fmul_rn(g.vz[k + 1], izv), a1);
+            atomicAdd(acc + k, __fmul_rn(p, __fsub_rn(mz, a0)));
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && s_ovf)
+    atomicExch(err, 2);
+  double ssq = 0.0;
+  const i64 base = i64(col) * g.nz;
+  for (int z = threadIdx.x; z < g.nz; z += blockDim.x) {
+    const float v = acc[z];
+    float o = v;
+    if (EPI == EPI_NORM) {
+      ssq += double(v) * double(v);
+    } else if (EPI == EPI_SIRT) {
+      const float t = __fadd_rn(e.x[base + z], __fmul_rn(1.0f, __fmul_rn(v, e.w[base + z])));
+      o = (t < 0.0f) ? 0.0f : t;
+    } else if (EPI == EPI_MLEM) {
+      const float t = __fmul_rn(e.x[base + z], __fmul_rn(e.w[base + z], v));
+      o = (t < 0.0f) ? 0.0f : t;
+    }
+    vol[base + z] = o;
+  }
+  if (EPI == EPI_NORM) {
+    __shared__ double red[kBpThreads / 32];
+    const double t = cta_sum<kBpThreads / 32>(ssq, red);
+    if (threadIdx.x == 0)
+      e.partials[blockIdx.x] = t;
+  }
+}
+
+} // namespace
+
+size_t cb_fp_smem(const Geom &g) {
+  return size_t(kFpWarps) * 2 * size_t(g.nx + g.ny + 2) * sizeof(float);
+}
+
+size_t cb_bp_smem(const Geom &g) {
+  return size_t(g.nz) * sizeof(float) +
+         size_t(kBpAngleChunk) * kBpMaxRaysPerAngle * (sizeof(int) + 2 * sizeof(float));
+}
+
+int cb_prepare(const Geom &g) {
+  const int fp = int(cb_fp_smem(g)), bp = int(cb_bp_smem(g));
+  cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
+  const void *fps[] = {(const void *)cb_fp_kernel<EPI_STORE>, (const void *)cb_fp_kernel<EPI_NORM>,
+                       (const void *)cb_fp_kernel<EPI_SIRT>, (const void *)cb_fp_kernel<EPI_MLEM>};
+  const void *bps[] = {(const void *)cb_bp_kernel<EPI_STORE>, (const void *)cb_bp_kernel<EPI_NORM>,
+                       (const void *)cb_bp_kernel<EPI_SIRT>, (const void *)cb_bp_kernel<EPI_MLEM>};
+  for (const void *f : fps)
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, fp) != cudaSuccess)
+      e1 = cudaErrorInvalidValue;
+  for (const void *f : bps)
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bp) != cudaSuccess)
+      e2 = cudaErrorInvalidValue;
+  return (e1 == cudaSuccess && e2 == cudaSuccess) ? 0 : 1;
+}
+
+int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
+               const int2 *hrange, int grid, cudaStream_t st) {
+  const size_t smem = cb_fp_smem(g);
+  const int cap = g.nx + g.ny + 2;
+  switch (mode) {
+  case EPI_STORE:
+    cb_fp_kernel<EPI_STORE><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap);
+    break;
+  case EPI_NORM:
+    cb_fp_kernel<EPI_NORM><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap);
+    break;
+  case EPI_SIRT:
+    cb_fp_kernel<EPI_SIRT><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap);
+    break;
+  case EPI_MLEM:
+    cb_fp_kernel<EPI_MLEM><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap);
+    break;
+  default:
+    return 1;
+  }
+  return 0;
+}
+
+int cb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
+                int *err, cudaStream_t st) {
+  const size_t smem = cb_bp_smem(g);
+  const int ncol = g.nx * g.ny;
+  switch (mode) {
+  case EPI_STORE:
+    cb_bp_kernel<EPI_STORE><<<ncol, kBpThreads, smem, st>>>(g, pix, vol, e, err);
+    break;
+  case EPI_NORM:
+    cb_bp_kernel<EPI_NORM><<<ncol, kBpThreads, smem, st>>>(g, pix, vol, e, err);
+    break;
+  case EPI_SIRT:
+    cb_bp_kernel<EPI_SIRT><<<ncol, kBpThreads, smem, st>>>(g, pix, vol, e, err);
+    break;
+  case EPI_MLEM:
+    cb_bp_kernel<EPI_MLEM><<<ncol, kBpThreads, smem, st>>>(g, pix, vol, e, err);
+    break;
+  default:
+    return 1;
+  }
+  return 0;
+}
+
+} // namespace ccpi

@@ -1,0 +1,90 @@
+// Shared device-side definitions for the B200 projectors and solvers.
+//
+// Data layout in HBM is the reference's (Core/src/base_types.hpp:45-63,
+// instruments.cpp:29-33): sinogram [angle][h][v] with detector rows v
+// fastest, volume [x][y][z] with z fastest.  The v/z axis is the lane axis
+// of every projector kernel, so warps read and write contiguous rows.
+//
+// Arithmetic that decides which voxels a ray visits, or that the reference
+// rounds in a particular order, is written with explicitly rounded
+// intrinsics (__dadd_rn, __fmul_rn, ...) and the projector translation units
+// are compiled with --fmad=false: the reference's x86-64 build never fuses a
+// multiply-add, and fusing would change both tie decisions and results.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ccpi {
+
+typedef long long i64;
+
+// Tie tolerance of both walks (p2D.cpp:20, c2D.cpp:15).
+constexpr float kEps = FLT_EPSILON;
+
+// Geometry of one problem as the kernels see it.  Plain data plus device
+// pointers to per-angle / per-pixel tables built on the host (cos/sin are
+// evaluated by the host C library, as the reference does, so angle tables
+// are identical bit for bit).
+struct Geom {
+  int kind; // 0 parallel beam, 1 cone beam
+  int na, nh, nv, nx, ny, nz;
+  double origin[3], size[3];
+  const double *cosA, *sinA; // na
+  const double *hpix, *vpix; // nh, nv
+  // ---- parallel beam (p2D.cpp)
+  double det_x;           // 2 * max |origin|
+  float d_conv;           // 3 * det_x, the ray's alpha span
+  double ihp, hp0;        // 1/pixel step, h_pixels[0]/step
+  const double *yoff, *ioff, *blen; // back-projector trapezoid tables (na)
+  int map_type;           // 1, 2, 4 rows per slice, 0 general
+  const int *map;         // nv: row -> slice
+  const int *vlo, *vhi;   // nz: rows [vlo, vhi) mapping to each slice
+  // ---- cone beam (c2D.cpp)
+  double src[3], detx;
+  double cl, cipix, chpix0; // det_x - src_x, 1/h step, (src_y - h0)/step
+  const double *p1x, *p1y, *cdx, *sdx; // na
+  const float *dconv;     // nh * nv source-pixel distance
+  const float *dz, *iz;   // nv: v_pix - src_z and its reciprocal
+  const float *vz;        // nz + 1: slice planes relative to src_z
+  float inv_dz, pzbz, pzbz1, pzdv, z1, znm, pzdeps;
+  int mid;                // first row above the source
+};
+
+// Epilogue operands shared by the fused projector epilogues.
+struct Epi {
+  const float *b;    // measured sinogram (SIRT/MLEM) or unused
+  const float *w;    // per-element weight: R (SIRT fp), C (SIRT bp), N (MLEM bp)
+  float *x;          // volume updated in place by the back-projector epilogues
+  double *partials;  // one FP64 partial sum of squares per CTA (NORM modes)
+};
+
+enum EpiMode {
+  EPI_STORE = 0, // out = A x
+  EPI_NORM = 1,  // out = A x, and per-CTA sum of squares in FP64
+  EPI_SIRT = 2,  // fp: r = (b - Ax) R       bp: x = max(x + C A^T r, 0)
+  EPI_MLEM = 3,  // fp: q = max(b / Ax, 0)   bp: x = max(x (N A^T q), 0)
+};
+
+__device__ __forceinline__ int warp_lane() { return threadIdx.x & 31; }
+
+// Deterministic CTA reduction of a double (fixed shuffle/smem order).
+template <int NWARPS>
+__device__ __forceinline__ double cta_sum(double v, double *scratch) {
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    scratch[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NWARPS; i++)
+      t += scratch[i];
+  }
+  __syncthreads();
+  return t;
+}
+
+} // namespace ccpi

@@ -1,0 +1,735 @@
+// Plans (device geometry tables), projector dispatch and the solver loops.
+//
+// Solvers restate Core/src/Algorithms/cgls.cpp (cgls_base + cgls_3d,
+// cgls_regularize), sirt.cpp and mlem.cpp.  Every iteration runs without a
+// host round trip: the CGLS step scalars live in device memory (FP64), the
+// SIRT/MLEM updates and the sums of squares are fused into the projector
+// epilogues, and one iteration is captured once as a CUDA graph and
+// replayed.  CCPI_SOLVE_PLAIN instead launches each iteration from the
+// host and reads the scalars back every iteration, the way a host-driven
+// port of the reference's loop runs; it is kept as the comparison path.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ccpi_b200.h"
+#include "engine.h"
+#include "kernels.h"
+
+ccpi_plan::~ccpi_plan() {
+  for (void *b : bufs)
+    cudaFree(b);
+}
+
+namespace ccpi {
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string &m) { g_last_error = m; }
+
+bool cuda_ok(cudaError_t e, const char *what) {
+  if (e == cudaSuccess)
+    return true;
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return false;
+}
+
+namespace {
+
+template <class T> T *upload(ccpi_plan *p, const std::vector<T> &h) {
+  if (h.empty())
+    return nullptr;
+  void *d = nullptr;
+  if (cudaMalloc(&d, h.size() * sizeof(T)) != cudaSuccess)
+    return nullptr;
+  p->bufs.push_back(d);
+  cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+  return static_cast<T *>(d);
+}
+
+bool evenly_increasing(const double *p, int n) {
+  for (int i = 1; i < n; i++)
+    if (!(p[i] > p[i - 1]))
+      return false;
+  return true;
+}
+
+} // namespace
+
+int plan_create(const ccpi_geometry *gi, ccpi_plan **out) {
+  *out = nullptr;
+  if (!gi || (gi->kind != CCPI_PARALLEL && gi->kind != CCPI_CONE)) {
+    set_error("ccpi_plan_create: geometry kind must be CCPI_PARALLEL or CCPI_CONE");
+    return 1;
+  }
+  if (gi->n_angles < 1 || gi->n_h < 2 || gi->n_v < 1 || gi->nx < 1 || gi->ny < 1 ||
+      gi->nz < 1 || !gi->angles || !gi->h_pixels || !gi->v_pixels) {
+    set_error("ccpi_plan_create: empty geometry (need >= 1 angle, >= 2 detector "
+              "columns, >= 1 row and a non-empty voxel grid)");
+    return 1;
+  }
+  if (!evenly_increasing(gi->h_pixels, gi->n_h) || !evenly_increasing(gi->v_pixels, gi->n_v)) {
+    set_error("ccpi_plan_create: detector coordinates must be increasing");
+    return 1;
+  }
+  for (int i = 0; i < 3; i++)
+    if (!(gi->voxel_size[i] > 0.0)) {
+      set_error("ccpi_plan_create: voxel sizes must be positive");
+      return 1;
+    }
+  if (i64(gi->nx) * gi->ny * gi->nz > (i64(1) << 40) ||
+      i64(gi->n_angles) * gi->n_h * gi->n_v > (i64(1) << 40)) {
+    set_error("ccpi_plan_create: problem too large");
+    return 1;
+  }
+  if (i64(gi->nx) * gi->ny >= (i64(1) << 31)) {
+    set_error("ccpi_plan_create: more than 2^31 voxel columns");
+    return 1;
+  }
+  ccpi_plan *p = new ccpi_plan();
+  cudaGetDevice(&p->device);
+  Geom &g = p->g;
+  std::memset(&g, 0, sizeof(g));
+  g.kind = gi->kind;
+  g.na = gi->n_angles;
+  g.nh = gi->n_h;
+  g.nv = gi->n_v;
+  g.nx = gi->nx;
+  g.ny = gi->ny;
+  g.nz = gi->nz;
+  for (int i = 0; i < 3; i++) {
+    g.origin[i] = gi->origin[i];
+    g.size[i] = gi->voxel_size[i];
+  }
+  p->nvox = i64(g.nx) * g.ny * g.nz;
+  p->npix = i64(g.na) * g.nh * g.nv;
+  const int na = g.na, nh = g.nh, nv = g.nv, nz = g.nz;
+  std::vector<double> ca(na), sa(na), hp(gi->h_pixels, gi->h_pixels + nh),
+      vp(gi->v_pixels, gi->v_pixels + nv);
+  for (int a = 0; a < na; a++) {
+    // the host C library's cos/sin, as the reference evaluates them
+    ca[a] = std::cos(gi->angles[a]);
+    sa[a] = std::sin(gi->angles[a]);
+  }
+  g.cosA = upload(p, ca);
+  g.sinA = upload(p, sa);
+  g.hpix = upload(p, hp);
+  g.vpix = upload(p, vp);
+  bool ok = g.cosA && g.sinA && g.hpix && g.vpix;
+  if (g.kind == CCPI_PARALLEL) {
+    // p2D.cpp:477-494 forward constants
+    g.det_x = 2.0 * std::max(std::abs(g.origin[0]),
+                             std::max(std::abs(g.origin[1]), std::abs(g.origin[2])));
+    g.d_conv = float(3.0 * g.det_x);
+    g.ihp = 1.0 / (hp[1] - hp[0]);
+    g.hp0 = hp[0] / (hp[1] - hp[0]);
+    // p2D.cpp:995-1049 per-angle trapezoid tables of the (0,0) voxel
+    std::vector<double> yoff(na), ioff(na), blen(na);
+    const double o0 = g.origin[0], o1 = g.origin[1], d0 = g.size[0], d1 = g.size[1];
+    for (int a = 0; a < na; a++) {
+      const double c = ca[a], s = sa[a];
+      const double y00 = o1 * c - o0 * s;
+      const double y01 = (o1 + d1) * c - o0 * s;
+      const double y10 = o1 * c - (o0 + d0) * s;
+      const double y11 = (o1 + d1) * c - (o0 + d0) * s;
+      double ymin, ybot;
+      if (c > 0.0) {
+        if (s > 0.0) {
+          ymin = y10;
+          ybot = (y11 < y00) ? y11 : y00;
+        } else {
+          ymin = y00;
+          ybot = (y01 < y10) ? y01 : y10;
+        }
+      } else {
+        if (s > 0.0) {
+          ymin = y11;
+          ybot = (y01 < y10) ? y01 : y10;
+        } else {
+          ymin = y01;
+          ybot = (y11 < y00) ? y11 : y00;
+        }
+      }
+      yoff[a] = ybot - ymin;
+      ioff[a] = 1.0 / yoff[a];
+      blen[a] = (std::abs(c) > std::abs(s)) ? d0 / std::abs(c) : d1 / std::abs(s);
+    }
+    g.yoff = upload(p, yoff);
+    g.ioff = upload(p, ioff);
+    g.blen = upload(p, blen);
+    // p2D.cpp:22-61 row -> slice mapping
+    std::vector<int> map(nv), vlo(nz, 0), vhi(nz, 0);
+    for (int v = 0; v < nv; v++)
+      map[v] = int(std::floor((vp[v] - g.origin[2]) / g.size[2]));
+    g.map_type = 0;
+    for (int per : {1, 2, 4}) {
+      bool same = true;
+      for (int v = 0; v < nv && same; v++)
+        same = map[v] == v / per;
+      // the fast paths index the column without a bound: rows must land in it
+      if (same && map[nv - 1] < nz) {
+        g.map_type = per;
+        break;
+      }
+    }
+    // rows of each slice, in row order (the mapping is non-decreasing)
+    for (int z = 0; z < nz; z++) {
+      vlo[z] = nv;
+      vhi[z] = nv;
+    }
+    for (int v = nv - 1; v >= 0; v--)
+      if (map[v] >= 0 && map[v] < nz) {
+        if (vhi[map[v]] == nv && vlo[map[v]] == nv)
+          vhi[map[v]] = v + 1;
+        vlo[map[v]] = v;
+      }
+    for (int z = 0; z < nz; z++)
+      if (vlo[z] == nv)
+        vhi[z] = nv;
+    g.map = upload(p, map);
+    g.vlo = upload(p, vlo);
+    g.vhi = upload(p, vhi);
+    ok = ok && g.yoff && g.ioff && g.blen && g.map && g.vlo && g.vhi;
+    p->fp_grid = int(std::min<i64>((i64(na) * nh + 3) / 4, 148 * 16));
+    p->bp_parts = pb_bp_tiles(g);
+  } else {
+    if (nv < 2) {
+      set_error("ccpi_plan_create: cone beam needs at least 2 detector rows");
+      delete p;
+      return 1;
+    }
+    const double sx = gi->source[0], sy = gi->source[1], sz = gi->source[2];
+    g.src[0] = sx;
+    g.src[1] = sy;
+    g.src[2] = sz;
+    g.detx = gi->detector_x;
+    // c2D.cpp:480-492: first row above the source
+    g.mid = -1;
+    for (int i = 0; i < nv; i++)
+      if (vp[i] > sz) {
+        g.mid = i;
+        break;
+      }
+    if (g.mid <= 0) {
+      set_error("ccpi_plan_create: the source height must lie strictly inside the "
+                "detector's row range");
+      delete p;
+      return 1;
+    }
+    g.cl = g.detx - sx;
+    const double step = hp[1] - hp[0];
+    g.cipix = 1.0 / step;
+    g.chpix0 = (sy - hp[0]) / step;
+    std::vector<double> p1x(na), p1y(na), cdx(na), sdx(na);
+    for (int a = 0; a < na; a++) {
+      p1x[a] = ca[a] * sx - sa[a] * sy;
+      p1y[a] = sa[a] * sx + ca[a] * sy;
+      cdx[a] = ca[a] * g.detx;
+      sdx[a] = sa[a] * g.detx;
+    }
+    g.p1x = upload(p, p1x);
+    g.p1y = upload(p, p1y);
+    g.cdx = upload(p, cdx);
+    g.sdx = upload(p, sdx);
+    // c2D.cpp:495-516 and :993-1010 tables
+    std::vector<float> dconv(size_t(nh) * nv), dz(nv), iz(nv), vz(nz + 1);
+    const double x2 = (g.detx - sx) * (g.detx - sx);
+    for (int i = 0; i < nh; i++) {
+      const double xy2 = x2 + (hp[i] - sy) * (hp[i] - sy);
+      for (int j = 0; j < nv; j++)
+        dconv[size_t(i) * nv + j] = float(std::sqrt(xy2 + (vp[j] - sz) * (vp[j] - sz)));
+    }
+    for (int i = 0; i < nv; i++) {
+      dz[i] = float(vp[i] - sz);
+      iz[i] = float(1.0 / double(dz[i]));
+    }
+    for (int i = 0; i <= nz; i++)
+      vz[i] = float(g.origin[2] + double(i) * g.size[2] - sz);
+    g.dconv = upload(p, dconv);
+    g.dz = upload(p, dz);
+    g.iz = upload(p, iz);
+    g.vz = upload(p, vz);
+    g.inv_dz = float(1.0 / g.size[2]);
+    g.pzbz = float((sz - g.origin[2]) / g.size[2]);
+    g.pzbz1 = float(double(g.pzbz) + 1.0);
+    const double v_step = vp[1] - vp[0];
+    g.pzdv = float((sz - vp[0]) / v_step);
+    g.z1 = float((g.origin[2] + g.size[2] - sz) / v_step);
+    g.znm = float((g.origin[2] + double(nz - 1) * g.size[2] - sz) / v_step);
+    g.pzdeps = float(double(g.pzdv) * (1.0 + double(kEps)));
+    // c2D.cpp:558-600: detector columns that can see the whole volume
+    std::vector<int2> hr(na);
+    const double x0 = g.origin[0], xn = g.origin[0] + double(g.nx) * g.size[0];
+    const double y0 = g.origin[1], yn = g.origin[1] + double(g.ny) * g.size[1];
+    for (int a = 0; a < na; a++) {
+      const double c = ca[a], s = sa[a];
+      const double dx0 = x0 - p1x[a], dy0 = y0 - p1y[a], dxn = xn - p1x[a], dyn = yn - p1y[a];
+      const double cx0 = c * x0 - sx, cxn = c * xn - sx, sy0 = s * y0, syn = s * yn;
+      double y00, y01, y10, y11;
+      if (std::abs(s) > std::abs(c)) {
+        const double il = g.cl / s;
+        y00 = (c - dx0 / (sy0 + cx0)) * il;
+        y01 = (c - dx0 / (syn + cx0)) * il;
+        y10 = (c - dxn / (sy0 + cxn)) * il;
+        y11 = (c - dxn / (syn + cxn)) * il;
+      } else {
+        const double il = g.cl / c;
+        y00 = (-s + dy0 / (cx0 + sy0)) * il;
+        y01 = (-s + dyn / (cx0 + syn)) * il;
+        y10 = (-s + dy0 / (cxn + sy0)) * il;
+        y11 = (-s + dyn / (cxn + syn)) * il;
+      }
+      const int h00 = int(std::floor(y00 * g.cipix + g.chpix0));
+      const int h01 = int(std::floor(y01 * g.cipix + g.chpix0));
+      const int h10 = int(std::floor(y10 * g.cipix + g.chpix0));
+      const int h11 = int(std::floor(y11 * g.cipix + g.chpix0));
+      hr[a].x = std::max(std::min(std::min(h00, h01), std::min(h10, h11)), 0);
+      hr[a].y = std::min(std::max(std::max(h00, h01), std::max(h10, h11)), nh - 1);
+    }
+    p->hrange = upload(p, hr);
+    ok = ok && g.p1x && g.p1y && g.cdx && g.sdx && g.dconv && g.dz && g.iz && g.vz &&
+         p->hrange;
+    if (cb_fp_smem(g) > 200 * 1024 || cb_bp_smem(g) > 200 * 1024) {
+      set_error("ccpi_plan_create: volume too large for the cone kernels' shared memory");
+      delete p;
+      return 1;
+    }
+    ok = ok && cb_prepare(g) == 0;
+    p->fp_grid = int(std::min<i64>((i64(na) * nh + 3) / 4, 148 * 8));
+    p->bp_parts = g.nx * g.ny;
+  }
+  void *err = nullptr;
+  ok = ok && cudaMalloc(&err, sizeof(int)) == cudaSuccess;
+  if (err) {
+    p->bufs.push_back(err);
+    p->err = static_cast<int *>(err);
+    cudaMemset(err, 0, sizeof(int));
+  }
+  if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
+    set_error(std::string("ccpi_plan_create: device allocation or copy failed: ") +
+              cudaGetErrorString(cudaGetLastError()));
+    delete p;
+    return 2;
+  }
+  *out = p;
+  return 0;
+}
+
+int forward(const ccpi_plan *p, const float *vol, float *pix, int mode, const Epi &e,
+            cudaStream_t st) {
+  if (p->g.kind == CCPI_PARALLEL)
+    return pb_forward(p->g, vol, pix, mode, e, p->fp_grid, st);
+  return cb_forward(p->g, vol, pix, mode, e, p->hrange, p->fp_grid, st);
+}
+
+int backward(const ccpi_plan *p, const float *pix, float *vol, int mode, const Epi &e,
+             cudaStream_t st) {
+  if (p->g.kind == CCPI_PARALLEL)
+    return pb_backward(p->g, pix, vol, mode, e, p->err, st);
+  return cb_backward(p->g, pix, vol, mode, e, p->err, st);
+}
+
+// ------------------------------------------------------------------ solvers
+namespace {
+
+struct Work {
+  float *r = nullptr, *d = nullptr, *q = nullptr, *s = nullptr, *t = nullptr, *u = nullptr;
+  double *part1 = nullptr, *part2 = nullptr, *scal = nullptr, *norms = nullptr;
+};
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Workspace layout per algorithm (floats V = volume, P = sinogram):
+//  CGLS      r:P  d:V  q(Ad):P  s:V
+//  SIRT      r:P  d(C):V  q(R):P
+//  MLEM      r:P  d(N):V
+//  CGLS-reg  r:P  d:V  q(Adp):P  s:V  t(Adv):V  u:V
+size_t layout(const ccpi_plan *p, int alg, int niter, char *base, Work *w) {
+  const size_t V = size_t(p->nvox) * 4, P = size_t(p->npix) * 4;
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> char * {
+    char *q = base ? base + off : nullptr;
+    off += align_up(bytes);
+    return q;
+  };
+  Work tmp;
+  Work &W = w ? *w : tmp;
+  W.r = (float *)take(P);
+  W.d = (float *)take(V);
+  if (alg == CCPI_CGLS || alg == CCPI_SIRT || alg >= CCPI_CGLS_TIKHONOV)
+    W.q = (float *)take(P);
+  if (alg == CCPI_CGLS || alg >= CCPI_CGLS_TIKHONOV)
+    W.s = (float *)take(V);
+  if (alg >= CCPI_CGLS_TIKHONOV) {
+    W.t = (float *)take(V);
+    W.u = (float *)take(V);
+  }
+  const int nparts = std::max(std::max(p->fp_grid, p->bp_parts), sumsq_blocks());
+  W.part1 = (double *)take(sizeof(double) * nparts);
+  W.part2 = (double *)take(sizeof(double) * nparts);
+  W.scal = (double *)take(sizeof(double) * 8);
+  W.norms = (double *)take(sizeof(double) * std::max(niter, 1));
+  return off;
+}
+
+// One iteration of `alg` (kernels only; capturable).
+int iterate(const ccpi_plan *p, int alg, const float *sino, float *x, const Work &W,
+            float lambda, cudaStream_t st) {
+  const i64 V = p->nvox, P = p->npix;
+  Epi e{};
+  int rc = 0;
+  switch (alg) {
+  case CCPI_CGLS:
+    e.partials = W.part1;
+    rc |= forward(p, W.d, W.q, EPI_NORM, e, st);
+    k_cgls_scalars(S_ALPHA, W.part1, p->fp_grid, nullptr, 0, W.scal, nullptr, st);
+    k_axpy_scalar(W.r, W.q, P, W.scal, 1, -1.0f, st);
+    e.partials = W.part2;
+    rc |= backward(p, W.r, W.s, EPI_NORM, e, st);
+    k_cgls_scalars(S_BETA, W.part2, p->bp_parts, nullptr, 0, W.scal, W.norms, st);
+    k_cgls_xd(x, W.d, W.s, V, W.scal, st);
+    break;
+  case CCPI_SIRT:
+    e.b = sino;
+    e.w = W.q; // R
+    rc |= forward(p, x, W.r, EPI_SIRT, e, st);
+    e.w = W.d; // C
+    e.x = x;
+    rc |= backward(p, W.r, x, EPI_SIRT, e, st);
+    break;
+  case CCPI_MLEM:
+    e.b = sino;
+    rc |= forward(p, x, W.r, EPI_MLEM, e, st);
+    e.w = W.d; // N
+    e.x = x;
+    rc |= backward(p, W.r, x, EPI_MLEM, e, st);
+    break;
+  case CCPI_CGLS_TIKHONOV:
+  case CCPI_CGLS_TV:
+    e.partials = W.part1;
+    rc |= forward(p, W.d, W.q, EPI_NORM, e, st);
+    k_reg_accumulate(alg, W.d, W.t, p->g.nx, p->g.ny, p->g.nz, lambda, W.part2,
+                     sumsq_blocks(), st);
+    k_cgls_scalars(S_ALPHA2, W.part1, p->fp_grid, W.part2, sumsq_blocks(), W.scal, nullptr,
+                   st);
+    k_axpy_scalar(W.r, W.q, P, W.scal, 1, -1.0f, st);
+    k_add_scaled(W.u, x, W.d, V, W.scal, st);
+    k_reg_step(alg, W.u, x, p->g.nx, p->g.ny, p->g.nz, lambda, st);
+    e.partials = W.part2;
+    rc |= backward(p, W.r, W.s, EPI_NORM, e, st);
+    k_cgls_scalars(S_BETA, W.part2, p->bp_parts, nullptr, 0, W.scal, W.norms, st);
+    k_cgls_d(W.d, W.s, V, W.scal, st);
+    break;
+  default:
+    return 1;
+  }
+  return rc;
+}
+
+// Set-up before the first iteration (kernels only).
+int prepare(const ccpi_plan *p, int alg, const float *sino, float *x, const Work &W,
+            cudaStream_t st) {
+  const i64 V = p->nvox, P = p->npix;
+  Epi e{};
+  int rc = 0;
+  cudaMemsetAsync(W.scal, 0, sizeof(double) * 8, st);
+  switch (alg) {
+  case CCPI_CGLS:
+  case CCPI_CGLS_TIKHONOV:
+  case CCPI_CGLS_TV:
+    // the residual starts at b even for a warm start (cgls.cpp:33-46)
+    cudaMemcpyAsync(W.r, sino, size_t(P) * 4, cudaMemcpyDeviceToDevice, st);
+    e.partials = W.part2;
+    rc |= backward(p, W.r, W.d, EPI_NORM, e, st);
+    k_cgls_scalars(S_INIT, W.part2, p->bp_parts, nullptr, 0, W.scal, nullptr, st);
+    if (alg != CCPI_CGLS)
+      cudaMemsetAsync(W.t, 0, size_t(V) * 4, st);
+    break;
+  case CCPI_SIRT:
+    // R = 1 / (A 1), C = 1 / (A^T 1), non-positive -> 0 (sirt.cpp:31-48)
+    k_fill(W.d, V, 1.0f, st);
+    rc |= forward(p, W.d, W.q, EPI_STORE, e, st);
+    k_invert_pos(W.q, P, st);
+    k_fill(W.r, P, 1.0f, st);
+    rc |= backward(p, W.r, W.d, EPI_STORE, e, st);
+    k_invert_pos(W.d, V, st);
+    break;
+  case CCPI_MLEM:
+    // x = 1; N = 1 / (A^T 1), zeros kept (mlem.cpp:30-41)
+    k_fill(x, V, 1.0f, st);
+    k_fill(W.r, P, 1.0f, st);
+    rc |= backward(p, W.r, W.d, EPI_STORE, e, st);
+    k_invert_nonzero(W.d, V, st);
+    break;
+  default:
+    return 1;
+  }
+  return rc;
+}
+
+bool check_err(const ccpi_plan *p) {
+  int h = 0;
+  cudaMemcpy(&h, p->err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (h) {
+    cudaMemset(p->err, 0, sizeof(int));
+    set_error(h == 1 ? "projector: more detector columns per voxel than the back "
+                       "projector stages (voxel much larger than a pixel)"
+                     : "projector: cone back projector ray list overflow (voxel "
+                       "shadow wider than 24 detector columns)");
+    return false;
+  }
+  return true;
+}
+
+} // namespace
+
+size_t solve_workspace_bytes(const ccpi_plan *p, int alg, int niter) {
+  return layout(p, alg, niter, nullptr, nullptr);
+}
+
+// ---- sessions: one prepared solver whose iteration is a captured graph
+struct Session {
+  const ccpi_plan *plan = nullptr;
+  int alg = 0;
+  const float *sino = nullptr;
+  float *x = nullptr;
+  float lambda = 0.0f;
+  int flags = 0;
+  int max_iter = 0, done = 0;
+  cudaStream_t st = nullptr;
+  void *ws = nullptr;
+  Work W;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~Session() {
+    if (exec)
+      cudaGraphExecDestroy(exec);
+    if (graph)
+      cudaGraphDestroy(graph);
+    if (ws)
+      cudaFree(ws);
+  }
+};
+
+void *session_create(const ccpi_plan *p, int alg, const float *sino, float *x, double lambda,
+                     int max_iter, int flags, cudaStream_t st, int *rc) {
+  *rc = 0;
+  if (alg < CCPI_CGLS || alg > CCPI_CGLS_TV || max_iter < 0) {
+    set_error("ccpi_session_create: unknown algorithm or negative iteration budget");
+    *rc = 1;
+    return nullptr;
+  }
+  Session *S = new Session();
+  S->plan = p;
+  S->alg = alg;
+  S->sino = sino;
+  S->x = x;
+  S->lambda = float(lambda);
+  S->flags = flags;
+  S->max_iter = max_iter;
+  S->st = st;
+  const size_t need = layout(p, alg, max_iter, nullptr, nullptr);
+  if (!cuda_ok(cudaMalloc(&S->ws, need), "ccpi_session_create: workspace")) {
+    delete S;
+    *rc = 2;
+    return nullptr;
+  }
+  layout(p, alg, max_iter, static_cast<char *>(S->ws), &S->W);
+  *rc = prepare(p, alg, sino, x, S->W, st);
+  if (*rc == 0 && !(flags & CCPI_SOLVE_PLAIN)) {
+    bool ok = cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
+                      "ccpi_session_create: begin capture");
+    if (ok) {
+      *rc |= iterate(p, alg, sino, x, S->W, S->lambda, st);
+      ok = cuda_ok(cudaStreamEndCapture(st, &S->graph), "ccpi_session_create: end capture");
+    }
+    ok = ok && cuda_ok(cudaGraphInstantiate(&S->exec, S->graph, 0),
+                       "ccpi_session_create: instantiate");
+    if (!ok)
+      *rc |= 4;
+  }
+  if (*rc) {
+    delete S;
+    return nullptr;
+  }
+  return S;
+}
+
+int session_run(void *h, int n) {
+  Session *S = static_cast<Session *>(h);
+  if (n < 0 || S->done + n > S->max_iter) {
+    set_error("ccpi_session_run: iteration budget of the session exceeded");
+    return 1;
+  }
+  int rc = 0;
+  for (int it = 0; it < n && rc == 0; it++) {
+    if (S->flags & CCPI_SOLVE_PLAIN) {
+      double scal[8];
+      rc |= iterate(S->plan, S->alg, S->sino, S->x, S->W, S->lambda, S->st);
+      cudaMemcpyAsync(scal, S->W.scal, sizeof(scal), cudaMemcpyDeviceToHost, S->st);
+      cudaStreamSynchronize(S->st);
+    } else if (!cuda_ok(cudaGraphLaunch(S->exec, S->st), "ccpi_session_run: graph launch")) {
+      rc = 4;
+    }
+  }
+  S->done += n;
+  return rc;
+}
+
+int session_finish(void *h, double *h_norms) {
+  Session *S = static_cast<Session *>(h);
+  k_clamp0(S->x, S->plan->nvox, S->st);
+  if (!cuda_ok(cudaStreamSynchronize(S->st), "ccpi_session_finish: execution"))
+    return 8;
+  if (!check_err(S->plan))
+    return 16;
+  if (h_norms && S->done > 0 && (S->alg == CCPI_CGLS || S->alg >= CCPI_CGLS_TIKHONOV))
+    cudaMemcpy(h_norms, S->W.norms, sizeof(double) * S->done, cudaMemcpyDeviceToHost);
+  return 0;
+}
+
+void session_destroy(void *h) { delete static_cast<Session *>(h); }
+
+int solve(const ccpi_plan *p, int alg, const float *sino, float *x, int niter, double lambda,
+          double *h_norms, int flags, void *ws, size_t ws_bytes, cudaStream_t st) {
+  if (alg < CCPI_CGLS || alg > CCPI_CGLS_TV) {
+    set_error("ccpi_solve: unknown algorithm");
+    return 1;
+  }
+  if (niter < 0) {
+    set_error("ccpi_solve: negative iteration count");
+    return 1;
+  }
+  const size_t need = layout(p, alg, niter, nullptr, nullptr);
+  void *owned = nullptr;
+  if (!ws) {
+    if (!cuda_ok(cudaMalloc(&owned, need), "ccpi_solve: workspace allocation"))
+      return 2;
+    ws = owned;
+  } else if (ws_bytes < need) {
+    set_error("ccpi_solve: workspace too small");
+    return 1;
+  }
+  Work W;
+  layout(p, alg, niter, static_cast<char *>(ws), &W);
+  int rc = prepare(p, alg, sino, x, W, st);
+  const float lam = float(lambda);
+  if (flags & CCPI_SOLVE_PLAIN) {
+    double scal[8];
+    for (int it = 0; it < niter && rc == 0; it++) {
+      rc |= iterate(p, alg, sino, x, W, lam, st);
+      cudaMemcpyAsync(scal, W.scal, sizeof(scal), cudaMemcpyDeviceToHost, st);
+      cudaStreamSynchronize(st);
+    }
+  } else if (niter > 0 && rc == 0) {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
+                      "ccpi_solve: begin capture");
+    if (ok) {
+      rc |= iterate(p, alg, sino, x, W, lam, st);
+      ok = cuda_ok(cudaStreamEndCapture(st, &graph), "ccpi_solve: end capture");
+    }
+    ok = ok && cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "ccpi_solve: instantiate");
+    for (int it = 0; ok && it < niter; it++)
+      ok = cuda_ok(cudaGraphLaunch(exec, st), "ccpi_solve: graph launch");
+    if (exec)
+      cudaGraphExecDestroy(exec);
+    if (graph)
+      cudaGraphDestroy(graph);
+    if (!ok)
+      rc |= 4;
+  }
+  // every reconstruction is clamped at zero (voxels.cpp:187, :272, :352)
+  k_clamp0(x, p->nvox, st);
+  if (!cuda_ok(cudaStreamSynchronize(st), "ccpi_solve: execution"))
+    rc |= 8;
+  if (rc == 0 && !check_err(p))
+    rc = 16;
+  if (rc == 0 && h_norms && niter > 0 && (alg == CCPI_CGLS || alg >= CCPI_CGLS_TIKHONOV))
+    cudaMemcpy(h_norms, W.norms, sizeof(double) * niter, cudaMemcpyDeviceToHost);
+  if (owned)
+    cudaFree(owned);
+  if (rc && g_last_error.empty())
+    set_error("ccpi_solve: kernel launch failed");
+  return rc;
+}
+
+int solve_batched(int n, const ccpi_plan *const *plans, int alg, const float *const *sino,
+                  float *const *x, int niter, const double *lambda, cudaStream_t st) {
+  if (n <= 0)
+    return 0;
+  std::vector<void *> ws(n, nullptr);
+  std::vector<Work> W(n);
+  int rc = 0;
+  for (int i = 0; i < n && rc == 0; i++) {
+    const size_t need = layout(plans[i], alg, niter, nullptr, nullptr);
+    if (!cuda_ok(cudaMalloc(&ws[i], need), "ccpi_solve_batched: workspace"))
+      rc = 2;
+    else
+      layout(plans[i], alg, niter, static_cast<char *>(ws[i]), &W[i]);
+  }
+  // branches: problem i runs on stream i % kStreams inside the graph
+  const int kStreams = std::min(n, 16);
+  std::vector<cudaStream_t> br(kStreams, nullptr);
+  std::vector<cudaEvent_t> ev(kStreams + 1, nullptr);
+  for (int k = 0; k < kStreams && rc == 0; k++)
+    if (cudaStreamCreateWithFlags(&br[k], cudaStreamNonBlocking) != cudaSuccess)
+      rc = 2;
+  for (int k = 0; k <= kStreams && rc == 0; k++)
+    if (cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess)
+      rc = 2;
+  auto fork_join = [&](auto &&body) {
+    cudaEventRecord(ev[kStreams], st);
+    for (int k = 0; k < kStreams; k++)
+      cudaStreamWaitEvent(br[k], ev[kStreams], 0);
+    for (int i = 0; i < n; i++)
+      rc |= body(i, br[i % kStreams]);
+    for (int k = 0; k < kStreams; k++) {
+      cudaEventRecord(ev[k], br[k]);
+      cudaStreamWaitEvent(st, ev[k], 0);
+    }
+  };
+  if (rc == 0) {
+    fork_join([&](int i, cudaStream_t s) { return prepare(plans[i], alg, sino[i], x[i], W[i], s); });
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
+                      "ccpi_solve_batched: begin capture");
+    if (ok) {
+      fork_join([&](int i, cudaStream_t s) {
+        return iterate(plans[i], alg, sino[i], x[i], W[i], float(lambda ? lambda[i] : 0.0), s);
+      });
+      ok = cuda_ok(cudaStreamEndCapture(st, &graph), "ccpi_solve_batched: end capture");
+    }
+    ok = ok && cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "ccpi_solve_batched: instantiate");
+    for (int it = 0; ok && it < niter; it++)
+      ok = cuda_ok(cudaGraphLaunch(exec, st), "ccpi_solve_batched: graph launch");
+    if (exec)
+      cudaGraphExecDestroy(exec);
+    if (graph)
+      cudaGraphDestroy(graph);
+    if (!ok)
+      rc |= 4;
+    for (int i = 0; i < n; i++)
+      k_clamp0(x[i], plans[i]->nvox, st);
+    if (!cuda_ok(cudaStreamSynchronize(st), "ccpi_solve_batched: execution"))
+      rc |= 8;
+    for (int i = 0; i < n && rc == 0; i++)
+      if (!check_err(plans[i]))
+        rc = 16;
+  }
+  for (auto s : br)
+    if (s)
+      cudaStreamDestroy(s);
+  for (auto e : ev)
+    if (e)
+      cudaEventDestroy(e);
+  for (auto w : ws)
+    if (w)
+      cudaFree(w);
+  return rc;
+}
+
+} // namespace ccpi

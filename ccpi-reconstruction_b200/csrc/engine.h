@@ -1,0 +1,44 @@
+// Internal engine interface shared by the C ABI (capi.cu) and engine.cu.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/ccpi_b200.h"
+#include "common.cuh"
+
+struct ccpi_plan {
+  ccpi::Geom g{};
+  int device = 0;
+  long long nvox = 0, npix = 0;
+  int fp_grid = 1;  // CTAs of the forward projector (= its partial sums)
+  int bp_parts = 1; // CTAs of the back projector (= its partial sums)
+  int2 *hrange = nullptr; // cone: detector columns seeing the volume, per angle
+  int *err = nullptr;     // device error flag set by the projectors
+  std::vector<void *> bufs;
+  ~ccpi_plan();
+};
+
+namespace ccpi {
+
+extern thread_local std::string g_last_error;
+void set_error(const std::string &m);
+bool cuda_ok(cudaError_t e, const char *what);
+
+int plan_create(const ccpi_geometry *g, ccpi_plan **out);
+int forward(const ccpi_plan *p, const float *vol, float *pix, int mode, const Epi &e,
+            cudaStream_t st);
+int backward(const ccpi_plan *p, const float *pix, float *vol, int mode, const Epi &e,
+             cudaStream_t st);
+size_t solve_workspace_bytes(const ccpi_plan *p, int alg, int niter);
+int solve(const ccpi_plan *p, int alg, const float *sino, float *x, int niter, double lambda,
+          double *h_norms, int flags, void *ws, size_t ws_bytes, cudaStream_t st);
+void *session_create(const ccpi_plan *p, int alg, const float *sino, float *x, double lambda,
+                     int max_iter, int flags, cudaStream_t st, int *rc);
+int session_run(void *s, int n);
+int session_finish(void *s, double *h_norms);
+void session_destroy(void *s);
+int solve_batched(int n, const ccpi_plan *const *plans, int alg, const float *const *sino,
+                  float *const *x, int niter, const double *lambda, cudaStream_t st);
+
+} // namespace ccpi

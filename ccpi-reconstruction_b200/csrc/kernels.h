@@ -1,0 +1,66 @@
+// Host-callable launchers for the device kernels (internal to the library).
+#pragma once
+
+#include "common.cuh"
+
+namespace ccpi {
+
+// projectors (pb_project.cu, cb_project.cu); out is overwritten
+int pb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
+               int grid, cudaStream_t st);
+int pb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
+                int *err, cudaStream_t st);
+int pb_bp_tiles(const Geom &g);
+int cb_prepare(const Geom &g);
+size_t cb_fp_smem(const Geom &g);
+size_t cb_bp_smem(const Geom &g);
+int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
+               const int2 *hrange, int grid, cudaStream_t st);
+int cb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
+                int *err, cudaStream_t st);
+
+// vector kernels (vec_ops.cu)
+void k_fill(float *p, i64 n, float v, cudaStream_t st);
+void k_invert_pos(float *p, i64 n, cudaStream_t st);    // p > 0 ? 1/p : 0
+void k_invert_nonzero(float *p, i64 n, cudaStream_t st); // p != 0 ? 1/p : p
+void k_clamp0(float *p, i64 n, cudaStream_t st);
+void k_sumsq_partials(const float *x, i64 n, double *partials, int nblocks, cudaStream_t st);
+int sumsq_blocks();
+
+// CGLS scalar updates from FP64 partials.  s[] layout: see solver.cpp.
+enum ScalarOp { S_INIT = 0, S_ALPHA = 1, S_ALPHA2 = 2, S_BETA = 3 };
+void k_cgls_scalars(int op, const double *p1, int n1, const double *p2, int n2, double *s,
+                    double *norms, cudaStream_t st);
+// y += sign * alpha * x   (alpha = s[idx])
+void k_axpy_scalar(float *y, const float *x, i64 n, const double *s, int idx, float sign,
+                   cudaStream_t st);
+// x += alpha d; d = s_vec + beta d
+void k_cgls_xd(float *x, float *d, const float *sv, i64 n, const double *s, cudaStream_t st);
+// d = s_vec + beta d
+void k_cgls_d(float *d, const float *sv, i64 n, const double *s, cudaStream_t st);
+// out = in + alpha * d   (alpha = s[1])
+void k_add_scaled(float *out, const float *in, const float *d, i64 n, const double *s,
+                  cudaStream_t st);
+
+// regularisers (vec_ops.cu).  alg 3 Tikhonov, 4 TV.
+// acc += lambda * L(a), with per-CTA FP64 sum of squares of the new acc
+void k_reg_accumulate(int alg, const float *a, float *acc, int nx, int ny, int nz,
+                      float lambda, double *partials, int nblocks, cudaStream_t st);
+// out = a + lambda * L(a)
+void k_reg_step(int alg, const float *a, float *out, int nx, int ny, int nz, float lambda,
+                cudaStream_t st);
+// out = L(a)
+void k_reg_apply(int alg, const float *a, float *out, int nx, int ny, int nz,
+                 cudaStream_t st);
+
+// numpy front-end layouts
+// (na, nv, nh) -> (na, nh, nv_pad) with rows [voff, voff + nv) holding data
+void k_pack_parallel(const float *in, float *out, int na, int nv, int nh, int nv_pad,
+                     int voff, cudaStream_t st);
+// (na, nh, nv) -> (na, nh, nv_pad)
+void k_pack_cone(const float *in, float *out, int na, int nh, int nv, int nv_pad, int voff,
+                 cudaStream_t st);
+// (na, nh, nv) -> (na, nv, nh)
+void k_unpack_parallel(const float *in, float *out, int na, int nh, int nv, cudaStream_t st);
+
+} // namespace ccpi

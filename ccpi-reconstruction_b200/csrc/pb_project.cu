@@ -1,0 +1,748 @@
+// Parallel-beam Siddon projectors for sm_100a.
+//
+// Forward (parallel_beam::f2D, Core/src/p2D.cpp:468-611): ray-driven.  One
+// warp owns one ray (angle a, detector column h) and its lanes own detector
+// rows v, so every voxel-column read and every sinogram write is a
+// contiguous, coalesced row (float4 per lane when the layout allows).  The
+// xy walk is warp-uniform and is evaluated exactly as the reference does:
+// the volume is cut into 32x32 xy blocks, blocks are visited in the
+// reference's (x-block, y-block) order, each block applies the reference's
+// detector-column range rule and is walked from its own entry point with
+// block-local alpha tables, ties within FLT_EPSILON advance both axes, and
+// lengths are rounded to float.  Per row the sum is accumulated in the same
+// order with unfused float multiply and add, so the result equals the
+// reference bit for bit.
+//
+// Backward (parallel_beam::b2D, p2D.cpp:950-1087 with bproject_ah
+// :775-948): a voxel-driven gather, the reference's own design.  A CTA owns
+// a tile of xy voxel columns; it first evaluates, per (column, angle), the
+// detector columns whose rays cross the voxel square and their exact
+// trapezoid chord weights (FP64 geometry, float weights), staged in shared
+// memory; then each thread owns (column, z) pairs and accumulates the
+// sinogram rows in angle-then-column order, as the reference does.  No
+// atomics.
+//
+// Both kernels take fused epilogues (EpiMode): the SIRT and MLEM updates and
+// the FP64 sum of squares CGLS needs are applied to each output element
+// before it is stored, so no extra pass over HBM is spent on them.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ccpi {
+namespace {
+
+constexpr int kBlock = 32; // the reference's xy block edge (p2D.cpp:498-499)
+
+// std::max / std::min semantics (first argument on ties).
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
+
+__device__ __forceinline__ i64 col_offset(const Geom &g, int x, int y) {
+  const i64 off = (i64(x) * g.ny + y) * g.nz;
+  return (off >= 0 && off < i64(g.nx) * g.ny * g.nz) ? off : -1;
+}
+
+// Detector columns that can see the xy box [vx,wx) x [vy,wy) (p2D.cpp:527-595;
+// the per-voxel form at :808-915 is the same rule).
+__device__ void pb_hrange(const Geom &g, double vx, double wx, double vy, double wy,
+                          double c, double s, int &hmin, int &hmax) {
+  const double eps = double(kEps);
+  hmin = 0;
+  hmax = g.nh - 1;
+  if (fabs(c) < eps) {
+    if (s < 0.0) {
+      hmin = int(floor(vx * g.ihp - g.hp0));
+      hmax = int(floor((wx - eps) * g.ihp - g.hp0));
+    } else {
+      hmin = int(ceil((-wx + eps) * g.ihp - g.hp0));
+      hmax = int(ceil((-vx) * g.ihp - g.hp0));
+    }
+    hmin = max(hmin, 0);
+    hmax = min(hmax, g.nh - 1);
+  } else if (fabs(s) < eps) {
+    if (c < 0.0) {
+      hmin = int(ceil((-wy + eps) * g.ihp - g.hp0));
+      hmax = int(ceil((-vy) * g.ihp - g.hp0));
+    } else {
+      hmin = int(floor(vy * g.ihp - g.hp0));
+      hmax = int(floor((wy - eps) * g.ihp - g.hp0));
+    }
+    hmin = max(hmin, 0);
+    hmax = min(hmax, g.nh - 1);
+  } else {
+    double ymin, ymax;
+    if (c > 0.0) {
+      if (s > 0.0) {
+        ymin = vy * c - wx * s;
+        ymax = wy * c - vx * s;
+      } else {
+        ymin = vy * c - vx * s;
+        ymax = wy * c - wx * s;
+      }
+    } else {
+      if (s > 0.0) {
+        ymin = wy * c - wx * s;
+        ymax = vy * c - vx * s;
+      } else {
+        ymin = wy * c - vx * s;
+        ymax = vy * c - wx * s;
+      }
+    }
+    hmin = (ymin < g.hpix[0]) ? 0 : int(floor(ymin * g.ihp - g.hp0));
+    hmax = min(int(floor(ymax * g.ihp - g.hp0)), g.nh - 1);
+  }
+}
+
+// Walk one non-axis-parallel ray through one block from the block's own
+// entry point (p2D.cpp:284-458), calling add(offset, length) per cell.
+template <class F>
+__device__ __forceinline__ void pb_walk_block(const Geom &g, double p2x, double p2y,
+                                              double c, double s, int bx0, int by0,
+                                              int nxb, int nyb, double vx, double vy,
+                                              F &add) {
+  const double eps = double(kEps);
+  const double dx = g.size[0], dy = g.size[1];
+  const double xn = vx + double(nxb) * dx, yn = vy + double(nyb) * dy;
+  const double ic = 1.0 / c, is = 1.0 / s;
+  const double ax0 = (vx - p2x) * ic, ay0 = (vy - p2y) * is;
+  const double axn = (xn - p2x) * ic, ayn = (yn - p2y) * is;
+  const double amin = dmax(dmax(dmin(ax0, axn), dmin(ay0, ayn)), double(-g.d_conv));
+  const double amax = dmin(dmin(dmax(ax0, axn), dmax(ay0, ayn)), 0.0);
+  if (!(amin < amax - eps))
+    return;
+  const int sx = c > 0.0 ? 1 : -1, sy = s > 0.0 ? 1 : -1;
+  int x = 0, y = 0;
+  const bool x_face_first = !(sx > 0 && sy < 0); // octant (+,-) tests y first
+  auto cx = [&]() { return int(floor((p2x + amin * c - vx) / dx)); };
+  auto cy = [&]() { return int(floor((p2y + amin * s - vy) / dy)); };
+  const double axe = sx > 0 ? ax0 : axn; // entry through the x face
+  const double aye = sy > 0 ? ay0 : ayn; // entry through the y face
+  if (x_face_first) {
+    if (amin == axe) {
+      x = sx > 0 ? 0 : nxb - 1;
+      if (sx < 0 && sy < 0 && amin == ayn)
+        y = nyb - 1;
+      else
+        y = cy();
+    } else if (amin == aye) {
+      x = cx();
+      y = sy > 0 ? 0 : nyb - 1;
+    }
+  } else {
+    if (amin == aye) {
+      x = cx();
+      y = nyb - 1;
+    } else if (amin == axe) {
+      x = 0;
+      y = cy();
+    }
+  }
+  double ap = amin;
+  while ((sx > 0 ? x < nxb : x >= 0) && (sy > 0 ? y < nyb : y >= 0)) {
+    const double nxa = (vx + double(sx > 0 ? x + 1 : x) * dx - p2x) * ic;
+    const double nya = (vy + double(sy > 0 ? y + 1 : y) * dy - p2y) * is;
+    const i64 off = col_offset(g, bx0 + x, by0 + y);
+    float len;
+    if (nxa < nya - eps) {
+      len = float(nxa - ap);
+      ap = nxa;
+      x += sx;
+    } else if (nya < nxa - eps) {
+      len = float(nya - ap);
+      ap = nya;
+      y += sy;
+    } else {
+      const double mx = dmax(nxa, nya);
+      len = float(mx - ap);
+      ap = mx;
+      x += sx;
+      y += sy;
+    }
+    add(off, len);
+  }
+}
+
+// All cells of ray (a, h) in the reference's accumulation order.
+template <class F>
+__device__ void pb_trace_ray(const Geom &g, int a, int h, F &add) {
+  const double eps = double(kEps);
+  const double c = g.cosA[a], s = g.sinA[a], hv = g.hpix[h];
+  const double p2x = c * g.det_x - s * hv;
+  const double p2y = s * g.det_x + c * hv;
+  const int nbx = (g.nx + kBlock - 1) / kBlock, nby = (g.ny + kBlock - 1) / kBlock;
+  const double dx = g.size[0], dy = g.size[1];
+  if (fabs(c) < eps && fabs(s) < eps)
+    return;
+  for (int bxi = 0; bxi < nbx; bxi++) {
+    const int bx0 = bxi * kBlock, nxb = min(kBlock, g.nx - bx0);
+    const double vx = g.origin[0] + double(bx0) * dx;
+    const double wx = g.origin[0] + double(bx0 + nxb) * dx;
+    int by_lo = 0, by_hi = nby - 1;
+    int ix = 0;
+    if (fabs(c) < eps) {
+      // parallel to y: the block column that holds the ray by the floor rule
+      ix = int(floor((p2x - vx) / dx));
+      if (ix < 0 || ix >= nxb)
+        continue;
+    } else if (!(fabs(s) < eps)) {
+      // prefilter: block rows the ray can cross inside this block column
+      const double t = s / c;
+      const double ya = p2y + (vx - p2x) * t, yb = p2y + (wx - p2x) * t;
+      const double margin = 1e-3 * dy;
+      const double ylo = fmin(ya, yb) - margin, yhi = fmax(ya, yb) + margin;
+      const double bsz = double(kBlock) * dy;
+      const double flo = floor((ylo - g.origin[1]) / bsz);
+      const double fhi = floor((yhi - g.origin[1]) / bsz);
+      if (fhi < 0.0 || flo > double(nby - 1))
+        continue;
+      by_lo = flo < 0.0 ? 0 : int(flo);
+      by_hi = fhi > double(nby - 1) ? nby - 1 : int(fhi);
+    }
+    for (int byi = by_lo; byi <= by_hi; byi++) {
+      const int by0 = byi * kBlock, nyb = min(kBlock, g.ny - by0);
+      const double vy = g.origin[1] + double(by0) * dy;
+      const double wy = g.origin[1] + double(by0 + nyb) * dy;
+      int hmin, hmax;
+      pb_hrange(g, vx, wx, vy, wy, c, s, hmin, hmax);
+      if (h < hmin || h > hmax)
+        continue;
+      if (fabs(c) < eps) {
+        const float len = float(dy);
+        for (int t = 0; t < nyb; t++) {
+          const int j = s < 0.0 ? nyb - 1 - t : t;
+          add(col_offset(g, bx0 + ix, by0 + j), len);
+        }
+      } else if (fabs(s) < eps) {
+        const int jy = int(floor((p2y - vy) / dy));
+        if (jy < 0 || jy >= nyb)
+          continue;
+        const float len = float(dx);
+        for (int t = 0; t < nxb; t++) {
+          const int i = c < 0.0 ? nxb - 1 - t : t;
+          add(col_offset(g, bx0 + i, by0 + jy), len);
+        }
+      } else {
+        pb_walk_block(g, p2x, p2y, c, s, bx0, by0, nxb, nyb, vx, vy, add);
+      }
+    }
+  }
+}
+
+template <int EPI>
+__device__ __forceinline__ float fp_epilogue(float acc, i64 idx, const Epi &e, double &ssq) {
+  if (EPI == EPI_NORM) {
+    ssq += double(acc) * double(acc);
+    return acc;
+  } else if (EPI == EPI_SIRT) {
+    // sirt.cpp:60-62: r = (-1) r + b, then r *= R
+    return __fmul_rn(__fadd_rn(-acc, e.b[idx]), e.w[idx]);
+  } else if (EPI == EPI_MLEM) {
+    // mlem.cpp:54,65 with blas.hpp div_xyz / clamp_min
+    const float q = (acc != 0.0f) ? __fdiv_rn(e.b[idx], acc) : 0.0f;
+    return (q < 0.0f) ? 0.0f : q;
+  }
+  return acc;
+}
+
+template <int NWARPS>
+__device__ void store_partial(double ssq, const Epi &e) {
+  __shared__ double red[NWARPS];
+  const double t = cta_sum<NWARPS>(ssq, red);
+  if (threadIdx.x == 0)
+    e.partials[blockIdx.x] = t;
+}
+
+// ---- forward, float4 rows (row v -> slice v, nv and nz multiples of 4)
+template <int NQ, int EPI>
+__global__ void __launch_bounds__(128) pb_fp_vec4(Geom g, const float *__restrict__ vol,
+                                                  float *__restrict__ pix, Epi e, int v0) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps_total = gridDim.x * (blockDim.x >> 5);
+  const int nrays = g.na * g.nh;
+  double ssq = 0.0;
+  for (int ray = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ray < nrays;
+       ray += nwarps_total) {
+    const int a = ray / g.nh, h = ray - a * g.nh;
+    float4 acc[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+      acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto add = [&](i64 off, float len) {
+      if (off < 0)
+        return;
+      const float *col = vol + off;
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        const int v = v0 + q * 128 + lane * 4;
+        if (v < g.nv) {
+          const float4 x = __ldg(reinterpret_cast<const float4 *>(col + v));
+          acc[q].x = __fadd_rn(acc[q].x, __fmul_rn(x.x, len));
+          acc[q].y = __fadd_rn(acc[q].y, __fmul_rn(x.y, len));
+          acc[q].z = __fadd_rn(acc[q].z, __fmul_rn(x.z, len));
+          acc[q].w = __fadd_rn(acc[q].w, __fmul_rn(x.w, len));
+        }
+      }
+    };
+    pb_trace_ray(g, a, h, add);
+    const i64 rbase = i64(ray) * g.nv;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      const int v = v0 + q * 128 + lane * 4;
+      if (v < g.nv) {
+        float4 o;
+        o.x = fp_epilogue<EPI>(acc[q].x, rbase + v + 0, e, ssq);
+        o.y = fp_epilogue<EPI>(acc[q].y, rbase + v + 1, e, ssq);
+        o.z = fp_epilogue<EPI>(acc[q].z, rbase + v + 2, e, ssq);
+        o.w = fp_epilogue<EPI>(acc[q].w, rbase + v + 3, e, ssq);
+        *reinterpret_cast<float4 *>(pix + rbase + v) = o;
+      }
+    }
+  }
+  if (EPI == EPI_NORM)
+    store_partial<4>(ssq, e);
+}
+
+// ---- forward, any row->slice mapping (p2D.cpp:63-213 cases 2, 4, default)
+template <int NS, int EPI>
+__global__ void __launch_bounds__(128) pb_fp_scalar(Geom g, const float *__restrict__ vol,
+                                                    float *__restrict__ pix, Epi e, int v0) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps_total = gridDim.x * (blockDim.x >> 5);
+  const int nrays = g.na * g.nh;
+  double ssq = 0.0;
+  int zmap[NS];
+#pragma unroll
+  for (int q = 0; q < NS; q++) {
+    const int v = v0 + q * 32 + lane;
+    zmap[q] = (v < g.nv) ? g.map[v] : -1;
+    if (zmap[q] >= g.nz)
+      zmap[q] = -1; // the reference reads past the column here
+  }
+  for (int ray = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ray < nrays;
+       ray += nwarps_total) {
+    const int a = ray / g.nh, h = ray - a * g.nh;
+    float acc[NS];
+#pragma unroll
+    for (int q = 0; q < NS; q++)
+      acc[q] = 0.f;
+    auto add = [&](i64 off, float len) {
+      if (off < 0)
+        return;
+#pragma unroll
+      for (int q = 0; q < NS; q++)
+        if (zmap[q] >= 0)
+          acc[q] = __fadd_rn(acc[q], __fmul_rn(__ldg(vol + off + zmap[q]), len));
+    };
+    pb_trace_ray(g, a, h, add);
+    const i64 rbase = i64(ray) * g.nv;
+#pragma unroll
+    for (int q = 0; q < NS; q++) {
+      const int v = v0 + q * 32 + lane;
+      if (v < g.nv)
+        pix[rbase + v] = fp_epilogue<EPI>(acc[q], rbase + v, e, ssq);
+    }
+  }
+  if (EPI == EPI_NORM)
+    store_partial<4>(ssq, e);
+}
+
+// ---- backward
+constexpr int kBpAngles = 16; // angles staged per pass
+constexpr int kBpMaxRays = 8; // detector columns per (voxel column, angle)
+
+struct BpEntry {
+  int h0, cnt;
+  float w[kBpMaxRays];
+};
+
+// Detector columns and chord weights of voxel column [x0,xn) x [y0,yn) at
+// angle a (bproject_ah, p2D.cpp:803-939).  Returns the count, or -1 when it
+// exceeds the staging capacity (reported as an error by the host).
+__device__ int pb_bp_rays(const Geom &g, double x0, double xn, double y0, double yn,
+                          int a, BpEntry &E) {
+  const double eps = double(kEps);
+  const double c = g.cosA[a], s = g.sinA[a];
+  int cnt = 0;
+  E.h0 = 0;
+  if (fabs(c) < eps || fabs(s) < eps) {
+    int hmin, hmax;
+    pb_hrange(g, x0, xn, y0, yn, c, s, hmin, hmax);
+    const bool par_y = fabs(c) < eps;
+    const double lo = par_y ? x0 : y0, hi = par_y ? xn : yn;
+    const bool neg = par_y ? !(s < 0.0) : (c < 0.0);
+    const float wt = float(par_y ? g.size[1] : g.size[0]);
+    for (int h = hmin; h <= hmax; h++) {
+      const double u = neg ? -g.hpix[h] : g.hpix[h];
+      if (u >= lo && u < hi) {
+        if (cnt == 0)
+          E.h0 = h;
+        else if (h != E.h0 + cnt)
+          return -1; // not contiguous: cannot happen for monotone pixels
+        if (cnt >= kBpMaxRays)
+          return -1;
+        E.w[cnt++] = wt;
+      }
+    }
+    return cnt;
+  }
+  double ymin, ymax;
+  if (c > 0.0) {
+    if (s > 0.0) {
+      ymin = y0 * c - xn * s;
+      ymax = yn * c - x0 * s;
+    } else {
+      ymin = y0 * c - x0 * s;
+      ymax = yn * c - xn * s;
+    }
+  } else {
+    if (s > 0.0) {
+      ymin = yn * c - xn * s;
+      ymax = y0 * c - x0 * s;
+    } else {
+      ymin = yn * c - x0 * s;
+      ymax = y0 * c - xn * s;
+    }
+  }
+  const int hmin = (ymin < g.hpix[0]) ? 0 : int(floor(ymin * g.ihp - g.hp0));
+  const int hmax = min(int(floor(ymax * g.ihp - g.hp0)), g.nh - 1);
+  const double ybot = ymin + g.yoff[a], ytop = ymax - g.yoff[a];
+  const double l = g.blen[a], io = g.ioff[a];
+  for (int h = hmin; h <= hmax; h++) {
+    if (h < 0)
+      continue;
+    const double hv = g.hpix[h];
+    if (!(hv > ymin + eps))
+      continue;
+    float wt;
+    if (hv < ybot)
+      wt = float(l * (hv - ymin) * io);
+    else if (hv <= ytop)
+      wt = float(l);
+    else if (hv < ymax - eps)
+      wt = float(l * (ymax - hv) * io);
+    else
+      break;
+    if (cnt == 0)
+      E.h0 = h;
+    if (cnt >= kBpMaxRays)
+      return -1;
+    E.w[cnt++] = wt;
+  }
+  return cnt;
+}
+
+template <int EPI>
+__device__ __forceinline__ float bp_epilogue(float acc, i64 idx, const Epi &e, double &ssq) {
+  if (EPI == EPI_NORM) {
+    ssq += double(acc) * double(acc);
+    return acc;
+  } else if (EPI == EPI_SIRT) {
+    // sirt.cpp:70-74: bp *= C; x += 1 * bp; x = max(x, 0)
+    const float v = __fadd_rn(e.x[idx], __fmul_rn(1.0f, __fmul_rn(acc, e.w[idx])));
+    return (v < 0.0f) ? 0.0f : v;
+  } else if (EPI == EPI_MLEM) {
+    // mlem.cpp:72-74: x *= (N * bp); x = max(x, 0)
+    const float v = __fmul_rn(e.x[idx], __fmul_rn(e.w[idx], acc));
+    return (v < 0.0f) ? 0.0f : v;
+  }
+  return acc;
+}
+
+// Stage the ray lists of this CTA's columns for angles [a0, a0 + kBpAngles).
+__device__ void pb_bp_stage(const Geom &g, int tx0, int ty0, int tw, int th, int a0,
+                            BpEntry *ent, int *err) {
+  const int ncol = tw * th;
+  for (int t = threadIdx.x; t < ncol * kBpAngles; t += blockDim.x) {
+    const int col = t / kBpAngles, ai = t - col * kBpAngles;
+    const int a = a0 + ai;
+    BpEntry E;
+    E.cnt = 0;
+    E.h0 = 0;
+    const int i = tx0 + col / th, j = ty0 + col % th;
+    if (a < g.na && i < g.nx && j < g.ny) {
+      const double x0 = g.origin[0] + double(i) * g.size[0];
+      const double xn = g.origin[0] + double(i + 1) * g.size[0];
+      const double y0 = g.origin[1] + double(j) * g.size[1];
+      const double yn = g.origin[1] + double(j + 1) * g.size[1];
+      const int n = pb_bp_rays(g, x0, xn, y0, yn, a, E);
+      if (n < 0) {
+        atomicExch(err, 1);
+        E.cnt = 0;
+      } else
+        E.cnt = n;
+    }
+    ent[t] = E;
+  }
+}
+
+// float4 over z (row v == slice z, nz % 4 == 0).  Each thread owns NP
+// (column, z-quad) pairs.
+template <int NP, int EPI>
+__global__ void __launch_bounds__(256) pb_bp_vec4(Geom g, const float *__restrict__ pix,
+                                                  float *__restrict__ vol, Epi e, int tw,
+                                                  int th, int *err) {
+  extern __shared__ BpEntry ent[];
+  const int ntx = (g.nx + tw - 1) / tw;
+  const int tx0 = (blockIdx.x % ntx) * tw, ty0 = (blockIdx.x / ntx) * th;
+  const int nzq = g.nz >> 2;
+  const int npairs = tw * th * nzq;
+  float4 acc[NP];
+  int pcol[NP], pq[NP];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int p = threadIdx.x + k * blockDim.x;
+    pcol[k] = (p < npairs) ? p / nzq : -1;
+    pq[k] = (p < npairs) ? p - (p / nzq) * nzq : 0;
+  }
+  for (int a0 = 0; a0 < g.na; a0 += kBpAngles) {
+    __syncthreads();
+    pb_bp_stage(g, tx0, ty0, tw, th, a0, ent, err);
+    __syncthreads();
+    const int na_chunk = min(kBpAngles, g.na - a0);
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      if (pcol[k] < 0)
+        continue;
+      const BpEntry *E = ent + pcol[k] * kBpAngles;
+      for (int ai = 0; ai < na_chunk; ai++) {
+        const int cnt = E[ai].cnt;
+        const float *row =
+            pix + (i64(a0 + ai) * g.nh + E[ai].h0) * g.nv + pq[k] * 4;
+        for (int r = 0; r < cnt; r++) {
+          const float w = E[ai].w[r];
+          const float4 p = __ldg(reinterpret_cast<const float4 *>(row + i64(r) * g.nv));
+          acc[k].x = __fadd_rn(acc[k].x, __fmul_rn(p.x, w));
+          acc[k].y = __fadd_rn(acc[k].y, __fmul_rn(p.y, w));
+          acc[k].z = __fadd_rn(acc[k].z, __fmul_rn(p.z, w));
+          acc[k].w = __fadd_rn(acc[k].w, __fmul_rn(p.w, w));
+        }
+      }
+    }
+  }
+  double ssq = 0.0;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    if (pcol[k] < 0)
+      continue;
+    const int i = tx0 + pcol[k] / th, j = ty0 + pcol[k] % th;
+    if (i >= g.nx || j >= g.ny)
+      continue;
+    const i64 base = (i64(i) * g.ny + j) * g.nz + pq[k] * 4;
+    float4 o;
+    o.x = bp_epilogue<EPI>(acc[k].x, base + 0, e, ssq);
+    o.y = bp_epilogue<EPI>(acc[k].y, base + 1, e, ssq);
+    o.z = bp_epilogue<EPI>(acc[k].z, base + 2, e, ssq);
+    o.w = bp_epilogue<EPI>(acc[k].w, base + 3, e, ssq);
+    *reinterpret_cast<float4 *>(vol + base) = o;
+  }
+  if (EPI == EPI_NORM)
+    store_partial<8>(ssq, e);
+}
+
+// Scalar over z, any row->slice mapping (calc_ah_z cases, p2D.cpp:613-773).
+template <int NP, int EPI>
+__global__ void __launch_bounds__(256) pb_bp_scalar(Geom g, const float *__restrict__ pix,
+                                                    float *__restrict__ vol, Epi e, int tw,
+                                                    int th, int *err) {
+  extern __shared__ BpEntry ent[];
+  const int ntx = (g.nx + tw - 1) / tw;
+  const int tx0 = (blockIdx.x % ntx) * tw, ty0 = (blockIdx.x / ntx) * th;
+  const int npairs = tw * th * g.nz;
+  float acc[NP];
+  int pcol[NP], pz[NP];
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    acc[k] = 0.f;
+    const int p = threadIdx.x + k * blockDim.x;
+    pcol[k] = (p < npairs) ? p / g.nz : -1;
+    pz[k] = (p < npairs) ? p - (p / g.nz) * g.nz : 0;
+  }
+  for (int a0 = 0; a0 < g.na; a0 += kBpAngles) {
+    __syncthreads();
+    pb_bp_stage(g, tx0, ty0, tw, th, a0, ent, err);
+    __syncthreads();
+    const int na_chunk = min(kBpAngles, g.na - a0);
+#pragma unroll
+    for (int k = 0; k < NP; k++) {
+      if (pcol[k] < 0)
+        continue;
+      const int z = pz[k];
+      const BpEntry *E = ent + pcol[k] * kBpAngles;
+      for (int ai = 0; ai < na_chunk; ai++) {
+        const int cnt = E[ai].cnt;
+        const float *row = pix + (i64(a0 + ai) * g.nh + E[ai].h0) * g.nv;
+        for (int r = 0; r < cnt; r++) {
+          const float w = E[ai].w[r];
+          const float *p = row + i64(r) * g.nv;
+          switch (g.map_type) {
+          case 1:
+            if (z < g.nv)
+              acc[k] = __fadd_rn(acc[k], __fmul_rn(p[z], w));
+            break;
+          case 2:
+            if (2 * z + 1 < g.nv)
+              acc[k] = __fadd_rn(acc[k], __fmul_rn(__fadd_rn(p[2 * z], p[2 * z + 1]), w));
+            break;
+          case 4:
+            if (4 * z + 3 < g.nv) {
+              const float t = __fadd_rn(__fadd_rn(__fadd_rn(p[4 * z], p[4 * z + 1]), p[4 * z + 2]),
+                                        p[4 * z + 3]);
+              acc[k] = __fadd_rn(acc[k], __fmul_rn(t, w));
+            }
+            break;
+          default:
+            for (int v = g.vlo[z]; v < g.vhi[z]; v++)
+              acc[k] = __fadd_rn(acc[k], __fmul_rn(p[v], w));
+            break;
+          }
+        }
+      }
+    }
+  }
+  double ssq = 0.0;
+#pragma unroll
+  for (int k = 0; k < NP; k++) {
+    if (pcol[k] < 0)
+      continue;
+    const int i = tx0 + pcol[k] / th, j = ty0 + pcol[k] % th;
+    if (i >= g.nx || j >= g.ny)
+      continue;
+    const i64 idx = (i64(i) * g.ny + j) * g.nz + pz[k];
+    vol[idx] = bp_epilogue<EPI>(acc[k], idx, e, ssq);
+  }
+  if (EPI == EPI_NORM)
+    store_partial<8>(ssq, e);
+}
+
+template <int EPI>
+int launch_fp(const Geom &g, const float *vol, float *pix, const Epi &e, int grid,
+              cudaStream_t st) {
+  const bool vec4 = g.map_type == 1 && (g.nv % 4) == 0 && (g.nz % 4) == 0;
+  if (vec4) {
+    for (int v0 = 0; v0 < g.nv; v0 += 512) {
+      const int left = g.nv - v0;
+      if (left > 256)
+        pb_fp_vec4<4, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+      else if (left > 128)
+        pb_fp_vec4<2, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+      else
+        pb_fp_vec4<1, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+    }
+  } else {
+    for (int v0 = 0; v0 < g.nv; v0 += 256) {
+      const int left = g.nv - v0;
+      if (left > 128)
+        pb_fp_scalar<8, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+      else if (left > 32)
+        pb_fp_scalar<4, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+      else
+        pb_fp_scalar<1, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+    }
+  }
+  return 0;
+}
+
+template <int EPI, int NP>
+void launch_bp_np(const Geom &g, bool vec4, const float *pix, float *vol, const Epi &e,
+                  int tw, int th, int *err, cudaStream_t st) {
+  const int tiles = ((g.nx + tw - 1) / tw) * ((g.ny + th - 1) / th);
+  const size_t smem = sizeof(BpEntry) * tw * th * kBpAngles;
+  if (vec4) {
+    cudaFuncSetAttribute(pb_bp_vec4<NP, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(smem));
+    pb_bp_vec4<NP, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, tw, th, err);
+  } else {
+    cudaFuncSetAttribute(pb_bp_scalar<NP, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(smem));
+    pb_bp_scalar<NP, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, tw, th, err);
+  }
+}
+
+template <int EPI>
+int launch_bp(const Geom &g, const float *pix, float *vol, const Epi &e, int *err,
+              cudaStream_t st) {
+  const bool vec4 = g.map_type == 1 && g.nv == g.nz && (g.nz % 4) == 0;
+  const int per_col = vec4 ? g.nz / 4 : g.nz;
+  // column tile: enough (column, z) pairs to fill 256 threads, at most 16
+  // pairs per thread
+  int tw = 4, th = 4;
+  if (per_col * 16 < 256) {
+    tw = 8;
+    th = 8;
+  }
+  int np = (tw * th * per_col + 255) / 256;
+  while (np > 16 && tw * th > 1) {
+    if (tw >= th)
+      tw = (tw + 1) / 2;
+    else
+      th = (th + 1) / 2;
+    np = (tw * th * per_col + 255) / 256;
+  }
+  if (np > 16)
+    return 2; // more than 4096 slices per column: not supported
+  if (np <= 1)
+    launch_bp_np<EPI, 1>(g, vec4, pix, vol, e, tw, th, err, st);
+  else if (np <= 2)
+    launch_bp_np<EPI, 2>(g, vec4, pix, vol, e, tw, th, err, st);
+  else if (np <= 4)
+    launch_bp_np<EPI, 4>(g, vec4, pix, vol, e, tw, th, err, st);
+  else if (np <= 8)
+    launch_bp_np<EPI, 8>(g, vec4, pix, vol, e, tw, th, err, st);
+  else
+    launch_bp_np<EPI, 16>(g, vec4, pix, vol, e, tw, th, err, st);
+  return 0;
+}
+
+} // namespace
+
+int pb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
+               int grid, cudaStream_t st) {
+  switch (mode) {
+  case EPI_STORE:
+    return launch_fp<EPI_STORE>(g, vol, pix, e, grid, st);
+  case EPI_NORM:
+    return launch_fp<EPI_NORM>(g, vol, pix, e, grid, st);
+  case EPI_SIRT:
+    return launch_fp<EPI_SIRT>(g, vol, pix, e, grid, st);
+  case EPI_MLEM:
+    return launch_fp<EPI_MLEM>(g, vol, pix, e, grid, st);
+  }
+  return 1;
+}
+
+int pb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
+                int *err, cudaStream_t st) {
+  switch (mode) {
+  case EPI_STORE:
+    return launch_bp<EPI_STORE>(g, pix, vol, e, err, st);
+  case EPI_NORM:
+    return launch_bp<EPI_NORM>(g, pix, vol, e, err, st);
+  case EPI_SIRT:
+    return launch_bp<EPI_SIRT>(g, pix, vol, e, err, st);
+  case EPI_MLEM:
+    return launch_bp<EPI_MLEM>(g, pix, vol, e, err, st);
+  }
+  return 1;
+}
+
+int pb_bp_tiles(const Geom &g) {
+  const bool vec4 = g.map_type == 1 && g.nv == g.nz && (g.nz % 4) == 0;
+  const int per_col = vec4 ? g.nz / 4 : g.nz;
+  int tw = 4, th = 4;
+  if (per_col * 16 < 256) {
+    tw = 8;
+    th = 8;
+  }
+  int np = (tw * th * per_col + 255) / 256;
+  while (np > 16 && tw * th > 1) {
+    if (tw >= th)
+      tw = (tw + 1) / 2;
+    else
+      th = (th + 1) / 2;
+    np = (tw * th * per_col + 255) / 256;
+  }
+  return ((g.nx + tw - 1) / tw) * ((g.ny + th - 1) / th);
+}
+
+} // namespace ccpi

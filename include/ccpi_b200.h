@@ -1,0 +1,210 @@
+/* ccpi_b200.h -- C ABI of the B200-native CCPi iterative reconstruction path.
+ *
+ * One shared library (ccpi-reconstruction_b200/libccpi_b200.so) exports
+ * everything below.  Signatures use plain pointers, sizes and doubles only;
+ * CUDA streams are passed as `void *` (a cudaStream_t, NULL = the legacy
+ * default stream).  Every entry point returns 0 on success and a nonzero
+ * code on failure; ccpi_last_error() then holds a message (per thread).
+ *
+ * Layouts are the reference's:
+ *   parallel-beam numpy sinogram  (n_angles, n_v, n_h), float32
+ *   cone-beam numpy sinogram      (n_angles, n_h, n_v), float32
+ *   internal / device sinogram    (n_angles, n_h, n_v), v fastest
+ *   volume                        (nx, ny, nz), z fastest
+ * Angles are degrees at the reference-facing calls (read as float32, as the
+ * reference's wrappers read them) and radians in ccpi_geometry.
+ */
+#ifndef CCPI_B200_H
+#define CCPI_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CCPI_CGLS = 0,
+  CCPI_SIRT = 1,
+  CCPI_MLEM = 2,
+  CCPI_CGLS_TIKHONOV = 3,
+  CCPI_CGLS_TV = 4
+};
+
+enum { CCPI_PARALLEL = 0, CCPI_CONE = 1 };
+
+/* Solver flags. */
+enum {
+  CCPI_SOLVE_PLAIN = 1 /* host-driven loop, one launch sequence per
+                          iteration, host reads the step scalars back every
+                          iteration (no CUDA graph) */
+};
+
+/* Explicit projector geometry in the reference's frame
+ * (Core/src/instruments.hpp:22-143): rays of detector column h and row v
+ * at angle a; parallel beam uses h_pixels/v_pixels as detector coordinates,
+ * cone beam places the source at `source` and the detector plane at
+ * x = detector_x before rotation. */
+typedef struct ccpi_geometry {
+  int kind; /* CCPI_PARALLEL or CCPI_CONE */
+  int n_angles, n_h, n_v;
+  const double *angles;   /* n_angles, radians */
+  const double *h_pixels; /* n_h, increasing, evenly spaced */
+  const double *v_pixels; /* n_v, increasing, evenly spaced */
+  double source[3];       /* cone beam only */
+  double detector_x;      /* cone beam only */
+  double origin[3];       /* corner of voxel (0, 0, 0) */
+  double voxel_size[3];
+  int nx, ny, nz;
+} ccpi_geometry;
+
+typedef struct ccpi_plan ccpi_plan; /* device tables for one geometry */
+
+/* Message of the last failure on this thread ("" if none). */
+const char *ccpi_last_error(void);
+/* Library version as major * 10000 + minor * 100 + patch. */
+int ccpi_version(void);
+
+/* ---------------------------------------------------------------------
+ * Reference-facing calls (host buffers in, host buffers out).
+ * ------------------------------------------------------------------- */
+
+/* Voxel grid the parallel-beam path derives from a sinogram shape.
+ * Replaces Diamond::setup_experimental_geometry + calculate_block_sizes +
+ * Diamond::get_xy_size (Core/src/diamond.cpp:35-86, :479-501,
+ * Core/src/voxels.cpp:12-46).  dims = {nx, ny, nz, n_v_padded, v_offset}. */
+int ccpi_pb_grid(int n_angles, int n_v, int n_h, double rotation_centre,
+                 int pixels_per_voxel, int dims[5]);
+
+/* parallelbeam.alg.{cgls,sirt,mlem,cgls_conv,cgls_tikhonov,cgls_TVreg}
+ * and their *_step forms.  Replaces reconstruct_iter
+ * (Wrappers/Python/src/diamond_wrapper.cpp:53-137; *_step: :140-257).
+ * pixels: (n_angles, n_v, n_h); volume: nx*ny*nz floats (ccpi_pb_grid);
+ * x0: NULL, or the previous volume for the *_step forms; norms: NULL or
+ * niterations doubles receiving |A^T r| per iteration (CGLS family);
+ * nthreads is accepted and ignored (the work runs on the current GPU). */
+int ccpi_pb_reconstruct(int alg, const float *pixels, int n_angles, int n_v,
+                        int n_h, const float *angles_deg,
+                        double rotation_centre, int pixels_per_voxel,
+                        int niterations, int nthreads, int is_pixels_in_log,
+                        double regularize, const float *x0, double *norms,
+                        float *volume);
+
+/* parallelbeam.alg.pb_forward_project (diamond_wrapper.cpp:421-556):
+ * volume (vx, vy, vz) -> (n_angles, n_v_padded, max(vx, vy)).  With
+ * out == NULL only out_dims is filled. */
+int ccpi_pb_forward_project(const float *volume, int vx, int vy, int vz,
+                            const float *angles_deg, int n_angles,
+                            int resolution, float *out, int out_dims[3]);
+
+/* parallelbeam.alg.pb_backward_project (diamond_wrapper.cpp:633-757):
+ * stack (n_angles, n_v, n_h) -> volume on the ccpi_pb_grid grid. */
+int ccpi_pb_backward_project(const float *stack, int n_angles, int n_v,
+                             int n_h, const float *angles_deg,
+                             double rotation_center, int resolution,
+                             float *out, int out_dims[3]);
+
+/* Voxel grid and detector of the cone-beam numpy path
+ * (Core/src/Readers/xtek.cpp:57-129, :367-380, :760-798).
+ * dims = {nx, ny, nz, n_v_padded, v_offset};
+ * geom = {voxel size xy, voxel size z, origin x, y, z}. */
+int ccpi_cb_grid(int n_angles, int n_h, int n_v, int pixels_per_voxel,
+                 double source_to_sample, double source_to_detector,
+                 double pixel_h_size, double pixel_v_size,
+                 double mask_radius, int dims[5], double geom[5]);
+
+/* Centre-of-rotation search of the cone-beam path (Nikon_XTek::find_centre,
+ * xtek.cpp:671-758; T. Liu, Opt. Eng. 48(4) 046501, 2009) on the padded,
+ * log sinogram (n_angles, n_h, n_v_padded) of ccpi_cb_grid's geometry.
+ * Returns the source y offset the reference applies (*y_centre). */
+int ccpi_cb_find_centre(const float *sino, int n_angles, int n_h,
+                        int n_v_padded, const float *angles_deg,
+                        double source_to_sample, double source_to_detector,
+                        double pixel_h_size, double *y_centre);
+
+/* conebeam.alg.{cgls,sirt,mlem,cgls_conv,cgls_tikhonov,cgls_TVreg}.
+ * Replaces conebeam_reconstruct_iter
+ * (Wrappers/Python/src/conebeam_wrapper.cpp:14-121).
+ * pixels: (n_angles, n_h, n_v); volume: nx*ny*nz (ccpi_cb_grid). */
+int ccpi_cb_reconstruct(int alg, const float *pixels, int n_angles, int n_h,
+                        int n_v, const float *angles_deg,
+                        int pixels_per_voxel, double source_to_sample,
+                        double source_to_detector, double pixel_h_size,
+                        double pixel_v_size, double mask_radius,
+                        int niterations, int nthreads, int is_pixels_in_log,
+                        double regularize, double *norms, float *volume);
+
+/* conebeam.alg.create_sinogram (conebeam_wrapper.cpp:346-400): the cone
+ * forward projection of an explicit geometry; out (n_angles, n_h, n_v). */
+int ccpi_cb_create_sinogram(const ccpi_geometry *geometry,
+                            const float *volume, float *out);
+
+/* ---------------------------------------------------------------------
+ * Device-level calls (device buffers; asynchronous on `stream` unless
+ * stated).  Replace the core projector and solver entry points the
+ * wrappers above drive: parallel_beam::f2D / b2D (Core/src/p2D.cpp:468,
+ * :950), cone_beam::f2D / b2D (Core/src/c2D.cpp:469, :1052) and
+ * reconstruction_alg::reconstruct (Core/src/algorithms.hpp:13-20).
+ * ------------------------------------------------------------------- */
+
+/* Build the device tables of a geometry on the current device (blocking).
+ * The geometry's arrays are copied; the caller may free them. */
+int ccpi_plan_create(const ccpi_geometry *geometry, ccpi_plan **plan);
+void ccpi_plan_destroy(ccpi_plan *plan);
+/* Sizes of a plan's volume and sinogram in elements. */
+long long ccpi_plan_voxels(const ccpi_plan *plan);
+long long ccpi_plan_pixels(const ccpi_plan *plan);
+
+/* sino = A vol (overwritten). */
+int ccpi_forward(const ccpi_plan *plan, const float *d_volume, float *d_sino,
+                 void *stream);
+/* vol = A^T sino (overwritten). */
+int ccpi_backward(const ccpi_plan *plan, const float *d_sino, float *d_volume,
+                  void *stream);
+
+/* Device bytes ccpi_solve needs as workspace for `alg` and `niterations`. */
+size_t ccpi_solve_workspace_bytes(const ccpi_plan *plan, int alg,
+                                  int niterations);
+
+/* Run `alg` for `niterations` on the device.  d_x holds the starting volume
+ * (zeros for a plain call) and receives the clamped result; d_sino is the
+ * log sinogram (n_angles, n_h, n_v) and is not modified.  d_workspace may
+ * be NULL (the library allocates and frees it).  h_norms (NULL or
+ * niterations doubles) receives |A^T r| per CGLS-family iteration.  Blocks
+ * until done. */
+int ccpi_solve(const ccpi_plan *plan, int alg, const float *d_sino,
+               float *d_x, int niterations, double regularize,
+               double *h_norms, int flags, void *d_workspace,
+               size_t workspace_bytes, void *stream);
+
+/* Solve n independent problems (uneven sizes allowed) together: each
+ * iteration of all problems is one captured CUDA graph whose branches run
+ * concurrently.  regularize: n values (or NULL for 0).  Blocks until done. */
+int ccpi_solve_batched(int n, const ccpi_plan *const *plans, int alg,
+                       const float *const *d_sino, float *const *d_x,
+                       int niterations, const double *regularize,
+                       void *stream);
+
+/* A prepared solver for iteration-by-iteration control (the reference's
+ * reconstruction_alg::reconstruct loop of Core/src/Algorithms/cgls.cpp,
+ * sirt.cpp and mlem.cpp, split
+ * into set-up, iterations and the final clamp of voxels.cpp:187).
+ * create: allocates the workspace, runs the set-up (initial back
+ * projection / normalisations) and captures one iteration as a CUDA graph;
+ * run: enqueues niterations graph launches on the session's stream
+ * (asynchronous), at most max_iterations over the session's life;
+ * finish: clamps d_x at zero, waits, checks the projectors' error flag and
+ * copies the per-iteration |A^T r| (CGLS family) to h_norms (NULL or one
+ * double per iteration run). */
+typedef struct ccpi_session ccpi_session;
+int ccpi_session_create(const ccpi_plan *plan, int alg, const float *d_sino,
+                        float *d_x, double regularize, int max_iterations,
+                        int flags, void *stream, ccpi_session **session);
+int ccpi_session_run(ccpi_session *session, int niterations);
+int ccpi_session_finish(ccpi_session *session, double *h_norms);
+void ccpi_session_destroy(ccpi_session *session);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CCPI_B200_H */

@@ -1,0 +1,129 @@
+"""Solvers through the reference-facing API against the reference's golden
+reconstructions.
+
+SIRT and MLEM use only bit-exact projectors and float updates in the
+reference's order, so they are expected to equal the reference bit for bit.
+The CGLS family computes its step scalars from FP64 inner products (the
+reference sums them in float), so it is compared by relative L2 error
+against the reference and against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden, golden_names, max_rel, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def api_call(d, x0=None):
+    from ccpi.reconstruction.parallelbeam import alg
+    fn = {0: "cgls", 1: "sirt", 2: "mlem", 3: "cgls_tikhonov", 4: "cgls_TVreg"}[int(d["alg"])]
+    niter = int(d["niter"])
+    args = (d["pixels"], d["angles"], float(d.get("cor", 0.0)), int(d.get("ppv", 1)), niter, 1)
+    is_log = bool(d.get("is_log", 0))
+    if x0 is not None:
+        if fn in ("cgls", "sirt", "mlem"):
+            return getattr(alg, fn + "_step")(*args, is_log, x0)
+    if fn in ("cgls_tikhonov", "cgls_TVreg"):
+        return getattr(alg, fn)(*args, float(d["lam"]), np.zeros(niter), is_log)
+    return getattr(alg, fn)(*args, is_log)
+
+
+@pytest.mark.parametrize("name", golden_names("api_"))
+def test_parallel_api_vs_reference(name, cuda):
+    d = golden(name)
+    rec = api_call(d)
+    ref = d["out"]
+    assert rec.shape == ref.shape and rec.dtype == np.float32
+    if int(d["alg"]) in (1, 2):
+        assert np.array_equal(rec, ref), max_rel(rec, ref)
+    else:
+        # FP64 step scalars vs the reference's FP32 ones: compare with the
+        # FP64 oracle (the accurate answer) and bound the distance to the
+        # reference by the reference's own rounding error
+        pix = d["pixels"]
+        na, nv, nh = pix.shape
+        g, nvp, voff = O.parallel_api_geometry(na, nv, nh, d["angles"], float(d["cor"]),
+                                               int(d["ppv"]))
+        sino = O.parallel_api_sinogram(pix, nvp, voff, bool(d["is_log"]))
+        r64 = O.solve(g, int(d["alg"]), sino.astype(np.float64), int(d["niter"]),
+                      lam=float(d["lam"]), fp64=True)
+        e_gpu = rel_l2(rec, r64)
+        e_ref = rel_l2(ref, r64)
+        assert e_gpu <= 1e-4, (e_gpu, e_ref)
+        assert rel_l2(rec, ref) <= max(1e-4, 2.0 * e_ref)
+
+
+@pytest.mark.parametrize("name", golden_names("step_"))
+def test_parallel_step_forms(name, cuda):
+    d = golden(name)
+    rec = api_call(d, x0=d["x0"])
+    if int(d["alg"]) in (1, 2):
+        assert np.array_equal(rec, d["out"])
+    else:
+        assert rel_l2(rec, d["out"]) <= 5e-4
+
+
+@pytest.mark.parametrize("alg", [0, 1, 2, 3, 4])
+def test_plain_and_graph_paths_agree(alg, cuda):
+    import torch
+    from ccpi.reconstruction.device import parallel_plan
+    p = parallel_plan((40, 40, 8), 50, 44)
+    rng = np.random.default_rng(alg)
+    x_true = torch.from_numpy(rng.random(p.shape).astype(np.float32)).to(cuda)
+    sino = p.forward(x_true)
+    a = torch.zeros(p.shape, device=cuda)
+    b = torch.zeros(p.shape, device=cuda)
+    p.solve(alg, sino, a, 7, regularize=0.001)
+    p.solve(alg, sino, b, 7, regularize=0.001, plain=True)
+    assert torch.equal(a, b)
+
+
+def test_batched_equals_individual(cuda):
+    import torch
+    from ccpi.reconstruction.device import parallel_plan, solve_batched
+    rng = np.random.default_rng(9)
+    plans, sinos, singles = [], [], []
+    for i in range(5):
+        n, nz, na = int(rng.integers(16, 48)), int(rng.choice([4, 8])), int(rng.integers(20, 70))
+        p = parallel_plan((n, n, nz), na, int(1.5 * n))
+        x = torch.from_numpy(rng.random(p.shape).astype(np.float32)).to(cuda)
+        s = p.forward(x)
+        y = torch.zeros(p.shape, device=cuda)
+        p.solve(3, s, y, 6, regularize=0.002 * (i + 1))
+        plans.append(p)
+        sinos.append(s)
+        singles.append(y)
+    xs = [torch.zeros(p.shape, device=cuda) for p in plans]
+    solve_batched(plans, 3, sinos, xs, 6, regularize=[0.002 * (i + 1) for i in range(5)])
+    for a, b in zip(xs, singles):
+        assert torch.equal(a, b)
+
+
+def test_slices_batched_equal_per_slice(cuda):
+    """SIRT on a 3-D parallel problem equals SIRT run slice by slice."""
+    import torch
+    from ccpi.reconstruction.device import parallel_plan
+    rng = np.random.default_rng(11)
+    p3 = parallel_plan((32, 32, 8), 40, 40)
+    x = torch.from_numpy(rng.random(p3.shape).astype(np.float32)).to(cuda)
+    s = p3.forward(x)
+    full = torch.zeros(p3.shape, device=cuda)
+    p3.solve(1, s, full, 5)
+    p1 = parallel_plan((32, 32, 1), 40, 40)
+    for k in range(8):
+        sk = s[:, :, k:k + 1].contiguous()
+        xk = torch.zeros(p1.shape, device=cuda)
+        p1.solve(1, sk, xk, 5)
+        assert torch.equal(xk[:, :, 0], full[:, :, k])
+
+
+def test_cone_api_vs_reference(cuda):
+    from ccpi.reconstruction.conebeam import alg
+    d = golden("cb_centre")
+    rec = alg.cgls(d["sino"], d["angles"], np.zeros(1), np.zeros(1), 1, float(d["s2s"]),
+                   float(d["s2d"]), float(d["px"]), float(d["px"]), float(d["mask_radius"]),
+                   False, np.zeros(3, np.float32), np.zeros(3, np.float32), 3, 1, True)
+    assert rec.shape == d["cgls3"].shape
+    assert rel_l2(rec, d["cgls3"]) <= 1e-4
