@@ -482,6 +482,32 @@ bool check_err(const ccpi_plan *p) {
   return true;
 }
 
+// Capture one iteration into an executable graph.  Capture runs on a
+// private stream ordered after `st` (the caller's stream may be the legacy
+// default stream, which cannot be captured); the graph is launched on `st`.
+bool capture_iteration(const ccpi_plan *p, int alg, const float *sino, float *x, const Work &W,
+                       float lambda, cudaStream_t st, cudaGraph_t *graph, cudaGraphExec_t *exec,
+                       int *rc) {
+  cudaStream_t cap = nullptr;
+  cudaEvent_t ev = nullptr;
+  bool ok = cuda_ok(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "capture stream") &&
+            cuda_ok(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "capture event");
+  ok = ok && cuda_ok(cudaEventRecord(ev, st), "capture event record") &&
+       cuda_ok(cudaStreamWaitEvent(cap, ev, 0), "capture stream wait");
+  ok = ok && cuda_ok(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal),
+                     "begin capture");
+  if (ok) {
+    *rc |= iterate(p, alg, sino, x, W, lambda, cap);
+    ok = cuda_ok(cudaStreamEndCapture(cap, graph), "end capture");
+  }
+  ok = ok && cuda_ok(cudaGraphInstantiate(exec, *graph, 0), "graph instantiate");
+  if (ev)
+    cudaEventDestroy(ev);
+  if (cap)
+    cudaStreamDestroy(cap);
+  return ok;
+}
+
 } // namespace
 
 size_t solve_workspace_bytes(const ccpi_plan *p, int alg, int niter) {
@@ -538,15 +564,7 @@ void *session_create(const ccpi_plan *p, int alg, const float *sino, float *x, d
   layout(p, alg, max_iter, static_cast<char *>(S->ws), &S->W);
   *rc = prepare(p, alg, sino, x, S->W, st);
   if (*rc == 0 && !(flags & CCPI_SOLVE_PLAIN)) {
-    bool ok = cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
-                      "ccpi_session_create: begin capture");
-    if (ok) {
-      *rc |= iterate(p, alg, sino, x, S->W, S->lambda, st);
-      ok = cuda_ok(cudaStreamEndCapture(st, &S->graph), "ccpi_session_create: end capture");
-    }
-    ok = ok && cuda_ok(cudaGraphInstantiate(&S->exec, S->graph, 0),
-                       "ccpi_session_create: instantiate");
-    if (!ok)
+    if (!capture_iteration(p, alg, sino, x, S->W, S->lambda, st, &S->graph, &S->exec, rc))
       *rc |= 4;
   }
   if (*rc) {
@@ -625,13 +643,7 @@ int solve(const ccpi_plan *p, int alg, const float *sino, float *x, int niter, d
   } else if (niter > 0 && rc == 0) {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    bool ok = cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
-                      "ccpi_solve: begin capture");
-    if (ok) {
-      rc |= iterate(p, alg, sino, x, W, lam, st);
-      ok = cuda_ok(cudaStreamEndCapture(st, &graph), "ccpi_solve: end capture");
-    }
-    ok = ok && cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "ccpi_solve: instantiate");
+    bool ok = capture_iteration(p, alg, sino, x, W, lam, st, &graph, &exec, &rc);
     for (int it = 0; ok && it < niter; it++)
       ok = cuda_ok(cudaGraphLaunch(exec, st), "ccpi_solve: graph launch");
     if (exec)
@@ -680,28 +692,36 @@ int solve_batched(int n, const ccpi_plan *const *plans, int alg, const float *co
   for (int k = 0; k <= kStreams && rc == 0; k++)
     if (cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess)
       rc = 2;
-  auto fork_join = [&](auto &&body) {
-    cudaEventRecord(ev[kStreams], st);
+  auto fork_join = [&](cudaStream_t root, auto &&body) {
+    cudaEventRecord(ev[kStreams], root);
     for (int k = 0; k < kStreams; k++)
       cudaStreamWaitEvent(br[k], ev[kStreams], 0);
     for (int i = 0; i < n; i++)
       rc |= body(i, br[i % kStreams]);
     for (int k = 0; k < kStreams; k++) {
       cudaEventRecord(ev[k], br[k]);
-      cudaStreamWaitEvent(st, ev[k], 0);
+      cudaStreamWaitEvent(root, ev[k], 0);
     }
   };
+  cudaStream_t root = nullptr;
+  if (rc == 0 && !cuda_ok(cudaStreamCreateWithFlags(&root, cudaStreamNonBlocking),
+                          "ccpi_solve_batched: capture stream"))
+    rc = 2;
   if (rc == 0) {
-    fork_join([&](int i, cudaStream_t s) { return prepare(plans[i], alg, sino[i], x[i], W[i], s); });
+    fork_join(st, [&](int i, cudaStream_t s) { return prepare(plans[i], alg, sino[i], x[i], W[i], s); });
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    bool ok = cuda_ok(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
+    // capture on a private stream ordered after st (st may be the legacy
+    // default stream, which cannot be captured)
+    cudaEventRecord(ev[kStreams], st);
+    cudaStreamWaitEvent(root, ev[kStreams], 0);
+    bool ok = cuda_ok(cudaStreamBeginCapture(root, cudaStreamCaptureModeThreadLocal),
                       "ccpi_solve_batched: begin capture");
     if (ok) {
-      fork_join([&](int i, cudaStream_t s) {
+      fork_join(root, [&](int i, cudaStream_t s) {
         return iterate(plans[i], alg, sino[i], x[i], W[i], float(lambda ? lambda[i] : 0.0), s);
       });
-      ok = cuda_ok(cudaStreamEndCapture(st, &graph), "ccpi_solve_batched: end capture");
+      ok = cuda_ok(cudaStreamEndCapture(root, &graph), "ccpi_solve_batched: end capture");
     }
     ok = ok && cuda_ok(cudaGraphInstantiate(&exec, graph, 0), "ccpi_solve_batched: instantiate");
     for (int it = 0; ok && it < niter; it++)
@@ -723,6 +743,8 @@ int solve_batched(int n, const ccpi_plan *const *plans, int alg, const float *co
   for (auto s : br)
     if (s)
       cudaStreamDestroy(s);
+  if (root)
+    cudaStreamDestroy(root);
   for (auto e : ev)
     if (e)
       cudaEventDestroy(e);

@@ -94,8 +94,13 @@ def test_cone_random_geometries_vs_oracle(seed, cuda):
              source=g.source, detector_x=g.detector_x)
     vol = rng.random(g.shape).astype(np.float32)
     pix = rng.random(g.sino_shape).astype(np.float32)
-    assert np.array_equal(run(p, "forward", vol, cuda), O.forward(g, vol))
-    assert max_rel(run(p, "backward", pix, cuda), O.backward(g, pix)) <= TOL
+    # an odd detector puts a row exactly at the source height, where the
+    # reference's own arithmetic yields NaN (it reports "Oops"): same NaNs
+    assert np.array_equal(run(p, "forward", vol, cuda), O.forward(g, vol), equal_nan=True)
+    b_gpu, b_ref = run(p, "backward", pix, cuda), O.backward(g, pix)
+    ok = np.isfinite(b_ref)
+    assert np.array_equal(np.isfinite(b_gpu), ok)
+    assert max_rel(b_gpu[ok], b_ref[ok]) <= TOL
 
 
 @pytest.mark.parametrize("kind", ["parallel", "cone"])
