@@ -38,6 +38,11 @@ PHANTOM = (512, 512, 256)
 WORKLOAD = ("parallel-beam SIRT, 512x512x256 ellipse phantom (20/slice) projected at 720 "
             "angles onto 768x256 detector, reconstructed on the 768x768x256 grid, all 256 "
             "slices per step")
+# --small: the same workload shrunk for profiler captures (still larger
+# than L2: 94 MB sinogram, 134 MB volume)
+SMALL = dict(NA=360, NV=128, NH=512, PHANTOM=(344, 344, 128),
+             WORKLOAD="parallel-beam SIRT, 344x344x128 phantom, 360 angles, 512x128 detector, "
+                      "512x512x128 grid (profiling size)")
 
 
 def parse():
@@ -48,7 +53,13 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--small", action="store_true", help="profiling-size workload")
+    args = ap.parse_args()
+    if args.small:
+        g = globals()
+        for k, v in SMALL.items():
+            g[k] = v
+    return args
 
 
 def load_peaks():
@@ -164,7 +175,7 @@ def cpu_reference_sample(sino_np_log):
     import oracle as O
     if not O.reference_available():
         return None
-    idx = np.arange(0, NA, NA // 24)[:24]
+    idx = np.arange(0, NA, max(NA // 24, 1))[:24]
     rows = slice(NV // 2 - 2, NV // 2 + 2)
     ang = np.linspace(0.0, 180.0, NA, endpoint=False).astype(np.float32)[idx]
     pix = np.ascontiguousarray(np.transpose(sino_np_log[idx][:, :, rows], (0, 2, 1)))

@@ -69,6 +69,16 @@ enum EpiMode {
 
 __device__ __forceinline__ int warp_lane() { return threadIdx.x & 31; }
 
+// acc += x * w, element-wise, unfused (two roundings per element, as the
+// reference's x86-64 build computes it).  Scalar intrinsics on purpose: the
+// packed f32x2 pair was measured to lose this equality.
+__device__ __forceinline__ void axpy4(float4 &acc, const float4 x, float w) {
+  acc.x = __fadd_rn(acc.x, __fmul_rn(x.x, w));
+  acc.y = __fadd_rn(acc.y, __fmul_rn(x.y, w));
+  acc.z = __fadd_rn(acc.z, __fmul_rn(x.z, w));
+  acc.w = __fadd_rn(acc.w, __fmul_rn(x.w, w));
+}
+
 // Deterministic CTA reduction of a double (fixed shuffle/smem order).
 template <int NWARPS>
 __device__ __forceinline__ double cta_sum(double v, double *scratch) {

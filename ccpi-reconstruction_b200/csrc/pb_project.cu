@@ -37,11 +37,6 @@ constexpr int kBlock = 32; // the reference's xy block edge (p2D.cpp:498-499)
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }
 
-__device__ __forceinline__ i64 col_offset(const Geom &g, int x, int y) {
-  const i64 off = (i64(x) * g.ny + y) * g.nz;
-  return (off >= 0 && off < i64(g.nx) * g.ny * g.nz) ? off : -1;
-}
-
 // Detector columns that can see the xy box [vx,wx) x [vy,wy) (p2D.cpp:527-595;
 // the per-voxel form at :808-915 is the same rule).
 __device__ void pb_hrange(const Geom &g, double vx, double wx, double vy, double wy,
@@ -94,12 +89,16 @@ __device__ void pb_hrange(const Geom &g, double vx, double wx, double vy, double
 }
 
 // Walk one non-axis-parallel ray through one block from the block's own
-// entry point (p2D.cpp:284-458), calling add(offset, length) per cell.
+// entry point (p2D.cpp:284-458), calling emit(column, length) per cell.
+// column = gx * ny + gy, or -1 outside the volume (the reference forms the
+// same flattened offset (x * ny + y) * nz and reads it).  The next x and y boundary
+// alphas are kept between steps and only the one crossed is re-evaluated,
+// with the reference's formula (b + i d - p2) / cos.
 template <class F>
 __device__ __forceinline__ void pb_walk_block(const Geom &g, double p2x, double p2y,
                                               double c, double s, int bx0, int by0,
                                               int nxb, int nyb, double vx, double vy,
-                                              F &add) {
+                                              F &emit) {
   const double eps = double(kEps);
   const double dx = g.size[0], dy = g.size[1];
   const double xn = vx + double(nxb) * dx, yn = vy + double(nyb) * dy;
@@ -137,40 +136,60 @@ __device__ __forceinline__ void pb_walk_block(const Geom &g, double p2x, double 
       y = cy();
     }
   }
+  auto ax_at = [&](int i) { return (vx + double(i) * dx - p2x) * ic; };
+  auto ay_at = [&](int j) { return (vy + double(j) * dy - p2y) * is; };
+  const int ox = sx > 0 ? 1 : 0, oy = sy > 0 ? 1 : 0;
+  double nxa = ax_at(x + ox), nya = ay_at(y + oy);
+  double nxm = nxa - eps, nym = nya - eps;
   double ap = amin;
+  const int ncol = g.nx * g.ny;
+  const int cstep_x = sx * g.ny;
+  int col = (bx0 + x) * g.ny + (by0 + y);
   while ((sx > 0 ? x < nxb : x >= 0) && (sy > 0 ? y < nyb : y >= 0)) {
-    const double nxa = (vx + double(sx > 0 ? x + 1 : x) * dx - p2x) * ic;
-    const double nya = (vy + double(sy > 0 ? y + 1 : y) * dy - p2y) * is;
-    const i64 off = col_offset(g, bx0 + x, by0 + y);
+    const int here = (unsigned(col) < unsigned(ncol)) ? col : -1;
     float len;
-    if (nxa < nya - eps) {
+    if (nxa < nym) {
       len = float(nxa - ap);
       ap = nxa;
       x += sx;
-    } else if (nya < nxa - eps) {
+      col += cstep_x;
+      nxa = ax_at(x + ox);
+      nxm = nxa - eps;
+    } else if (nya < nxm) {
       len = float(nya - ap);
       ap = nya;
       y += sy;
+      col += sy;
+      nya = ay_at(y + oy);
+      nym = nya - eps;
     } else {
       const double mx = dmax(nxa, nya);
       len = float(mx - ap);
       ap = mx;
       x += sx;
       y += sy;
+      col += cstep_x + sy;
+      nxa = ax_at(x + ox);
+      nya = ay_at(y + oy);
+      nxm = nxa - eps;
+      nym = nya - eps;
     }
-    add(off, len);
+    emit(here, len);
   }
 }
 
-// All cells of ray (a, h) in the reference's accumulation order.
-template <class F>
-__device__ void pb_trace_ray(const Geom &g, int a, int h, F &add) {
+// All cells of ray (a, h) in the reference's accumulation order: blocks in
+// (x-block, y-block) order, each applying the detector-column range rule.
+// `room` is called before each block (it may flush staged cells).
+template <class F, class R>
+__device__ void pb_trace_ray(const Geom &g, int a, int h, F &emit, R &room) {
   const double eps = double(kEps);
   const double c = g.cosA[a], s = g.sinA[a], hv = g.hpix[h];
   const double p2x = c * g.det_x - s * hv;
   const double p2y = s * g.det_x + c * hv;
   const int nbx = (g.nx + kBlock - 1) / kBlock, nby = (g.ny + kBlock - 1) / kBlock;
   const double dx = g.size[0], dy = g.size[1];
+  const int ncol = g.nx * g.ny;
   if (fabs(c) < eps && fabs(s) < eps)
     return;
   for (int bxi = 0; bxi < nbx; bxi++) {
@@ -206,11 +225,13 @@ __device__ void pb_trace_ray(const Geom &g, int a, int h, F &add) {
       pb_hrange(g, vx, wx, vy, wy, c, s, hmin, hmax);
       if (h < hmin || h > hmax)
         continue;
+      room();
       if (fabs(c) < eps) {
         const float len = float(dy);
         for (int t = 0; t < nyb; t++) {
           const int j = s < 0.0 ? nyb - 1 - t : t;
-          add(col_offset(g, bx0 + ix, by0 + j), len);
+          const int col = (bx0 + ix) * g.ny + by0 + j;
+          emit(unsigned(col) < unsigned(ncol) ? col : -1, len);
         }
       } else if (fabs(s) < eps) {
         const int jy = int(floor((p2y - vy) / dy));
@@ -219,10 +240,11 @@ __device__ void pb_trace_ray(const Geom &g, int a, int h, F &add) {
         const float len = float(dx);
         for (int t = 0; t < nxb; t++) {
           const int i = c < 0.0 ? nxb - 1 - t : t;
-          add(col_offset(g, bx0 + i, by0 + jy), len);
+          const int col = (bx0 + i) * g.ny + by0 + jy;
+          emit(unsigned(col) < unsigned(ncol) ? col : -1, len);
         }
       } else {
-        pb_walk_block(g, p2x, p2y, c, s, bx0, by0, nxb, nyb, vx, vy, add);
+        pb_walk_block(g, p2x, p2y, c, s, bx0, by0, nxb, nyb, vx, vy, emit);
       }
     }
   }
@@ -252,43 +274,94 @@ __device__ void store_partial(double ssq, const Epi &e) {
     e.partials[blockIdx.x] = t;
 }
 
+// Staged cell lists: the warp-uniform walk emits (column, length) pairs into
+// the warp's slice of shared memory; the lanes then accumulate them in
+// order, four cells at a time with all loads issued before the adds.
+constexpr int kFpWarps = 4;
+constexpr int kListCap = 256; // staged cells per warp
+constexpr int kBlockCells = 72; // most cells one ray has in one 32x32 block
+
+struct Cell {
+  int col;
+  float len;
+};
+
 // ---- forward, float4 rows (row v -> slice v, nv and nz multiples of 4)
 template <int NQ, int EPI>
-__global__ void __launch_bounds__(128) pb_fp_vec4(Geom g, const float *__restrict__ vol,
-                                                  float *__restrict__ pix, Epi e, int v0) {
-  const int lane = threadIdx.x & 31;
-  const int nwarps_total = gridDim.x * (blockDim.x >> 5);
+__global__ void __launch_bounds__(kFpWarps * 32) pb_fp_vec4(Geom g, const float *__restrict__ vol,
+                                                            float *__restrict__ pix, Epi e, int v0) {
+  __shared__ Cell lists[kFpWarps][kListCap];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  Cell *L = lists[wib];
+  const int nwarps_total = gridDim.x * kFpWarps;
   const int nrays = g.na * g.nh;
+  bool vok[NQ];
+  int vq[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    vq[q] = v0 + q * 128 + lane * 4;
+    vok[q] = vq[q] < g.nv;
+  }
   double ssq = 0.0;
-  for (int ray = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ray < nrays;
-       ray += nwarps_total) {
+  for (int ray = blockIdx.x * kFpWarps + wib; ray < nrays; ray += nwarps_total) {
     const int a = ray / g.nh, h = ray - a * g.nh;
     float4 acc[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++)
       acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-    auto add = [&](i64 off, float len) {
-      if (off < 0)
-        return;
-      const float *col = vol + off;
+    int n = 0;
+    auto flush = [&]() {
+      __syncwarp();
+      int m = 0;
+      for (; m + 4 <= n; m += 4) {
+        Cell c4[4];
+        float4 x[4][NQ];
 #pragma unroll
-      for (int q = 0; q < NQ; q++) {
-        const int v = v0 + q * 128 + lane * 4;
-        if (v < g.nv) {
-          const float4 x = __ldg(reinterpret_cast<const float4 *>(col + v));
-          acc[q].x = __fadd_rn(acc[q].x, __fmul_rn(x.x, len));
-          acc[q].y = __fadd_rn(acc[q].y, __fmul_rn(x.y, len));
-          acc[q].z = __fadd_rn(acc[q].z, __fmul_rn(x.z, len));
-          acc[q].w = __fadd_rn(acc[q].w, __fmul_rn(x.w, len));
+        for (int j = 0; j < 4; j++) {
+          c4[j] = L[m + j];
+#pragma unroll
+          for (int q = 0; q < NQ; q++)
+            x[j][q] = (c4[j].col >= 0 && vok[q])
+                          ? __ldg(reinterpret_cast<const float4 *>(vol + i64(c4[j].col) * g.nz + vq[q]))
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
         }
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (c4[j].col >= 0) {
+#pragma unroll
+            for (int q = 0; q < NQ; q++)
+              axpy4(acc[q], x[j][q], c4[j].len);
+          }
       }
+      for (; m < n; m++) {
+        const Cell c1 = L[m];
+        if (c1.col < 0)
+          continue;
+#pragma unroll
+        for (int q = 0; q < NQ; q++)
+          if (vok[q])
+            axpy4(acc[q], __ldg(reinterpret_cast<const float4 *>(vol + i64(c1.col) * g.nz + vq[q])),
+                  c1.len);
+      }
+      __syncwarp();
+      n = 0;
     };
-    pb_trace_ray(g, a, h, add);
+    auto emit = [&](int col, float len) {
+      if (lane == 0)
+        L[n] = Cell{col, len};
+      n++;
+    };
+    auto room = [&]() {
+      if (n > kListCap - kBlockCells)
+        flush();
+    };
+    pb_trace_ray(g, a, h, emit, room);
+    flush();
     const i64 rbase = i64(ray) * g.nv;
 #pragma unroll
     for (int q = 0; q < NQ; q++) {
-      const int v = v0 + q * 128 + lane * 4;
-      if (v < g.nv) {
+      if (vok[q]) {
+        const int v = vq[q];
         float4 o;
         o.x = fp_epilogue<EPI>(acc[q].x, rbase + v + 0, e, ssq);
         o.y = fp_epilogue<EPI>(acc[q].y, rbase + v + 1, e, ssq);
@@ -299,15 +372,17 @@ __global__ void __launch_bounds__(128) pb_fp_vec4(Geom g, const float *__restric
     }
   }
   if (EPI == EPI_NORM)
-    store_partial<4>(ssq, e);
+    store_partial<kFpWarps>(ssq, e);
 }
 
 // ---- forward, any row->slice mapping (p2D.cpp:63-213 cases 2, 4, default)
 template <int NS, int EPI>
-__global__ void __launch_bounds__(128) pb_fp_scalar(Geom g, const float *__restrict__ vol,
-                                                    float *__restrict__ pix, Epi e, int v0) {
-  const int lane = threadIdx.x & 31;
-  const int nwarps_total = gridDim.x * (blockDim.x >> 5);
+__global__ void __launch_bounds__(kFpWarps * 32) pb_fp_scalar(Geom g, const float *__restrict__ vol,
+                                                              float *__restrict__ pix, Epi e, int v0) {
+  __shared__ Cell lists[kFpWarps][kListCap];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  Cell *L = lists[wib];
+  const int nwarps_total = gridDim.x * kFpWarps;
   const int nrays = g.na * g.nh;
   double ssq = 0.0;
   int zmap[NS];
@@ -318,22 +393,39 @@ __global__ void __launch_bounds__(128) pb_fp_scalar(Geom g, const float *__restr
     if (zmap[q] >= g.nz)
       zmap[q] = -1; // the reference reads past the column here
   }
-  for (int ray = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ray < nrays;
-       ray += nwarps_total) {
+  for (int ray = blockIdx.x * kFpWarps + wib; ray < nrays; ray += nwarps_total) {
     const int a = ray / g.nh, h = ray - a * g.nh;
     float acc[NS];
 #pragma unroll
     for (int q = 0; q < NS; q++)
       acc[q] = 0.f;
-    auto add = [&](i64 off, float len) {
-      if (off < 0)
-        return;
+    int n = 0;
+    auto flush = [&]() {
+      __syncwarp();
+      for (int m = 0; m < n; m++) {
+        const Cell c1 = L[m];
+        if (c1.col < 0)
+          continue;
+        const float *colp = vol + i64(c1.col) * g.nz;
 #pragma unroll
-      for (int q = 0; q < NS; q++)
-        if (zmap[q] >= 0)
-          acc[q] = __fadd_rn(acc[q], __fmul_rn(__ldg(vol + off + zmap[q]), len));
+        for (int q = 0; q < NS; q++)
+          if (zmap[q] >= 0)
+            acc[q] = __fadd_rn(acc[q], __fmul_rn(__ldg(colp + zmap[q]), c1.len));
+      }
+      __syncwarp();
+      n = 0;
     };
-    pb_trace_ray(g, a, h, add);
+    auto emit = [&](int col, float len) {
+      if (lane == 0)
+        L[n] = Cell{col, len};
+      n++;
+    };
+    auto room = [&]() {
+      if (n > kListCap - kBlockCells)
+        flush();
+    };
+    pb_trace_ray(g, a, h, emit, room);
+    flush();
     const i64 rbase = i64(ray) * g.nv;
 #pragma unroll
     for (int q = 0; q < NS; q++) {
@@ -343,7 +435,7 @@ __global__ void __launch_bounds__(128) pb_fp_scalar(Geom g, const float *__restr
     }
   }
   if (EPI == EPI_NORM)
-    store_partial<4>(ssq, e);
+    store_partial<kFpWarps>(ssq, e);
 }
 
 // ---- backward
@@ -351,7 +443,7 @@ constexpr int kBpAngles = 16; // angles staged per pass
 constexpr int kBpMaxRays = 8; // detector columns per (voxel column, angle)
 
 struct BpEntry {
-  int h0, cnt;
+  int h0, cnt; // first detector column and number of rays; row index = a * nh + h0
   float w[kBpMaxRays];
 };
 
@@ -475,25 +567,30 @@ __device__ void pb_bp_stage(const Geom &g, int tx0, int ty0, int tw, int th, int
   }
 }
 
-// float4 over z (row v == slice z, nz % 4 == 0).  Each thread owns NP
-// (column, z-quad) pairs.
-template <int NP, int EPI>
-__global__ void __launch_bounds__(256) pb_bp_vec4(Geom g, const float *__restrict__ pix,
-                                                  float *__restrict__ vol, Epi e, int tw,
-                                                  int th, int *err) {
+// Vector over z (row v == slice z): each thread owns NP (column, group of
+// VW consecutive slices) pairs, VW = 8 (two float4) or 4; groups are the
+// fastest index so the lanes of a warp share a column and read its
+// staged rays as broadcasts.
+template <int NP, int VW, int EPI>
+__global__ void __launch_bounds__(256) pb_bp_vec(Geom g, const float *__restrict__ pix,
+                                                 float *__restrict__ vol, Epi e, int tw, int th,
+                                                 int *err) {
   extern __shared__ BpEntry ent[];
+  constexpr int NF = VW / 4;
   const int ntx = (g.nx + tw - 1) / tw;
   const int tx0 = (blockIdx.x % ntx) * tw, ty0 = (blockIdx.x / ntx) * th;
-  const int nzq = g.nz >> 2;
-  const int npairs = tw * th * nzq;
-  float4 acc[NP];
-  int pcol[NP], pq[NP];
+  const int nzg = g.nz / VW;
+  const int npairs = tw * th * nzg;
+  float4 acc[NP][NF];
+  int pcol[NP], pz[NP];
 #pragma unroll
   for (int k = 0; k < NP; k++) {
-    acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int f = 0; f < NF; f++)
+      acc[k][f] = make_float4(0.f, 0.f, 0.f, 0.f);
     const int p = threadIdx.x + k * blockDim.x;
-    pcol[k] = (p < npairs) ? p / nzq : -1;
-    pq[k] = (p < npairs) ? p - (p / nzq) * nzq : 0;
+    pcol[k] = (p < npairs) ? p / nzg : -1;
+    pz[k] = (p < npairs) ? (p - (p / nzg) * nzg) * VW : 0;
   }
   for (int a0 = 0; a0 < g.na; a0 += kBpAngles) {
     __syncthreads();
@@ -505,17 +602,20 @@ __global__ void __launch_bounds__(256) pb_bp_vec4(Geom g, const float *__restric
       if (pcol[k] < 0)
         continue;
       const BpEntry *E = ent + pcol[k] * kBpAngles;
+      const float *base = pix + pz[k];
       for (int ai = 0; ai < na_chunk; ai++) {
         const int cnt = E[ai].cnt;
-        const float *row =
-            pix + (i64(a0 + ai) * g.nh + E[ai].h0) * g.nv + pq[k] * 4;
+        const int row0 = (a0 + ai) * g.nh + E[ai].h0;
         for (int r = 0; r < cnt; r++) {
           const float w = E[ai].w[r];
-          const float4 p = __ldg(reinterpret_cast<const float4 *>(row + i64(r) * g.nv));
-          acc[k].x = __fadd_rn(acc[k].x, __fmul_rn(p.x, w));
-          acc[k].y = __fadd_rn(acc[k].y, __fmul_rn(p.y, w));
-          acc[k].z = __fadd_rn(acc[k].z, __fmul_rn(p.z, w));
-          acc[k].w = __fadd_rn(acc[k].w, __fmul_rn(p.w, w));
+          const float4 *p = reinterpret_cast<const float4 *>(base + i64(row0 + r) * g.nv);
+          float4 x[NF];
+#pragma unroll
+          for (int f = 0; f < NF; f++)
+            x[f] = __ldg(p + f);
+#pragma unroll
+          for (int f = 0; f < NF; f++)
+            axpy4(acc[k][f], x[f], w);
         }
       }
     }
@@ -528,13 +628,16 @@ __global__ void __launch_bounds__(256) pb_bp_vec4(Geom g, const float *__restric
     const int i = tx0 + pcol[k] / th, j = ty0 + pcol[k] % th;
     if (i >= g.nx || j >= g.ny)
       continue;
-    const i64 base = (i64(i) * g.ny + j) * g.nz + pq[k] * 4;
-    float4 o;
-    o.x = bp_epilogue<EPI>(acc[k].x, base + 0, e, ssq);
-    o.y = bp_epilogue<EPI>(acc[k].y, base + 1, e, ssq);
-    o.z = bp_epilogue<EPI>(acc[k].z, base + 2, e, ssq);
-    o.w = bp_epilogue<EPI>(acc[k].w, base + 3, e, ssq);
-    *reinterpret_cast<float4 *>(vol + base) = o;
+    const i64 base = (i64(i) * g.ny + j) * g.nz + pz[k];
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      float4 o;
+      o.x = bp_epilogue<EPI>(acc[k][f].x, base + 4 * f + 0, e, ssq);
+      o.y = bp_epilogue<EPI>(acc[k][f].y, base + 4 * f + 1, e, ssq);
+      o.z = bp_epilogue<EPI>(acc[k][f].z, base + 4 * f + 2, e, ssq);
+      o.w = bp_epilogue<EPI>(acc[k][f].w, base + 4 * f + 3, e, ssq);
+      *reinterpret_cast<float4 *>(vol + base + 4 * f) = o;
+    }
   }
   if (EPI == EPI_NORM)
     store_partial<8>(ssq, e);
@@ -623,75 +726,90 @@ int launch_fp(const Geom &g, const float *vol, float *pix, const Epi &e, int gri
     for (int v0 = 0; v0 < g.nv; v0 += 512) {
       const int left = g.nv - v0;
       if (left > 256)
-        pb_fp_vec4<4, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+        pb_fp_vec4<4, EPI><<<grid, kFpWarps * 32, 0, st>>>(g, vol, pix, e, v0);
       else if (left > 128)
-        pb_fp_vec4<2, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+        pb_fp_vec4<2, EPI><<<grid, kFpWarps * 32, 0, st>>>(g, vol, pix, e, v0);
       else
-        pb_fp_vec4<1, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+        pb_fp_vec4<1, EPI><<<grid, kFpWarps * 32, 0, st>>>(g, vol, pix, e, v0);
     }
   } else {
     for (int v0 = 0; v0 < g.nv; v0 += 256) {
       const int left = g.nv - v0;
       if (left > 128)
-        pb_fp_scalar<8, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+        pb_fp_scalar<8, EPI><<<grid, kFpWarps * 32, 0, st>>>(g, vol, pix, e, v0);
       else if (left > 32)
-        pb_fp_scalar<4, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+        pb_fp_scalar<4, EPI><<<grid, kFpWarps * 32, 0, st>>>(g, vol, pix, e, v0);
       else
-        pb_fp_scalar<1, EPI><<<grid, 128, 0, st>>>(g, vol, pix, e, v0);
+        pb_fp_scalar<1, EPI><<<grid, kFpWarps * 32, 0, st>>>(g, vol, pix, e, v0);
     }
   }
   return 0;
 }
 
-template <int EPI, int NP>
-void launch_bp_np(const Geom &g, bool vec4, const float *pix, float *vol, const Epi &e,
-                  int tw, int th, int *err, cudaStream_t st) {
-  const int tiles = ((g.nx + tw - 1) / tw) * ((g.ny + th - 1) / th);
-  const size_t smem = sizeof(BpEntry) * tw * th * kBpAngles;
-  if (vec4) {
-    cudaFuncSetAttribute(pb_bp_vec4<NP, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         int(smem));
-    pb_bp_vec4<NP, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, tw, th, err);
-  } else {
-    cudaFuncSetAttribute(pb_bp_scalar<NP, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         int(smem));
-    pb_bp_scalar<NP, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, tw, th, err);
+// Column tile and pairs per thread for the back projector: enough
+// (column, slice group) pairs to fill 256 threads, at most 16 per thread.
+struct BpShape {
+  int vw, tw, th, np;
+};
+
+BpShape bp_shape(const Geom &g) {
+  BpShape b;
+  b.vw = 1;
+  if (g.map_type == 1 && g.nv == g.nz) {
+    if (g.nz % 8 == 0)
+      b.vw = 8;
+    else if (g.nz % 4 == 0)
+      b.vw = 4;
   }
+  const int per_col = g.nz / b.vw;
+  b.tw = 4;
+  b.th = 4;
+  if (per_col * 16 < 256) {
+    b.tw = 8;
+    b.th = 8;
+  }
+  b.np = (b.tw * b.th * per_col + 255) / 256;
+  while (b.np > (b.vw == 8 ? 8 : 16) && b.tw * b.th > 1) {
+    if (b.tw >= b.th)
+      b.tw = (b.tw + 1) / 2;
+    else
+      b.th = (b.th + 1) / 2;
+    b.np = (b.tw * b.th * per_col + 255) / 256;
+  }
+  return b;
+}
+
+template <int EPI, int NP>
+int launch_bp_np(const Geom &g, const BpShape &b, const float *pix, float *vol, const Epi &e,
+                 int *err, cudaStream_t st) {
+  const int tiles = ((g.nx + b.tw - 1) / b.tw) * ((g.ny + b.th - 1) / b.th);
+  const size_t smem = sizeof(BpEntry) * b.tw * b.th * kBpAngles;
+  if (b.vw == 8)
+    pb_bp_vec<NP, 8, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
+  else if (b.vw == 4)
+    pb_bp_vec<NP, 4, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
+  else
+    pb_bp_scalar<NP, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
+  return 0;
 }
 
 template <int EPI>
 int launch_bp(const Geom &g, const float *pix, float *vol, const Epi &e, int *err,
               cudaStream_t st) {
-  const bool vec4 = g.map_type == 1 && g.nv == g.nz && (g.nz % 4) == 0;
-  const int per_col = vec4 ? g.nz / 4 : g.nz;
-  // column tile: enough (column, z) pairs to fill 256 threads, at most 16
-  // pairs per thread
-  int tw = 4, th = 4;
-  if (per_col * 16 < 256) {
-    tw = 8;
-    th = 8;
-  }
-  int np = (tw * th * per_col + 255) / 256;
-  while (np > 16 && tw * th > 1) {
-    if (tw >= th)
-      tw = (tw + 1) / 2;
-    else
-      th = (th + 1) / 2;
-    np = (tw * th * per_col + 255) / 256;
-  }
-  if (np > 16)
+  const BpShape b = bp_shape(g);
+  if (b.np > 16)
     return 2; // more than 4096 slices per column: not supported
-  if (np <= 1)
-    launch_bp_np<EPI, 1>(g, vec4, pix, vol, e, tw, th, err, st);
-  else if (np <= 2)
-    launch_bp_np<EPI, 2>(g, vec4, pix, vol, e, tw, th, err, st);
-  else if (np <= 4)
-    launch_bp_np<EPI, 4>(g, vec4, pix, vol, e, tw, th, err, st);
-  else if (np <= 8)
-    launch_bp_np<EPI, 8>(g, vec4, pix, vol, e, tw, th, err, st);
-  else
-    launch_bp_np<EPI, 16>(g, vec4, pix, vol, e, tw, th, err, st);
-  return 0;
+  if (b.np <= 1)
+    return launch_bp_np<EPI, 1>(g, b, pix, vol, e, err, st);
+  if (b.np <= 2)
+    return launch_bp_np<EPI, 2>(g, b, pix, vol, e, err, st);
+  if (b.np <= 4)
+    return launch_bp_np<EPI, 4>(g, b, pix, vol, e, err, st);
+  if (b.np <= 8)
+    return launch_bp_np<EPI, 8>(g, b, pix, vol, e, err, st);
+  if (b.vw == 8)
+    return 2;
+  return launch_bp_np<EPI, 16>(g, b, pix, vol, e, err, st);
 }
 
 } // namespace
@@ -727,22 +845,8 @@ int pb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi
 }
 
 int pb_bp_tiles(const Geom &g) {
-  const bool vec4 = g.map_type == 1 && g.nv == g.nz && (g.nz % 4) == 0;
-  const int per_col = vec4 ? g.nz / 4 : g.nz;
-  int tw = 4, th = 4;
-  if (per_col * 16 < 256) {
-    tw = 8;
-    th = 8;
-  }
-  int np = (tw * th * per_col + 255) / 256;
-  while (np > 16 && tw * th > 1) {
-    if (tw >= th)
-      tw = (tw + 1) / 2;
-    else
-      th = (th + 1) / 2;
-    np = (tw * th * per_col + 255) / 256;
-  }
-  return ((g.nx + tw - 1) / tw) * ((g.ny + th - 1) / th);
+  const BpShape b = bp_shape(g);
+  return ((g.nx + b.tw - 1) / b.tw) * ((g.ny + b.th - 1) / b.th);
 }
 
 } // namespace ccpi
