@@ -39,10 +39,10 @@ WORKLOAD = ("parallel-beam SIRT, 512x512x256 ellipse phantom (20/slice) projecte
             "angles onto 768x256 detector, reconstructed on the 768x768x256 grid, all 256 "
             "slices per step")
 # --small: the same workload shrunk for profiler captures (still larger
-# than L2: 94 MB sinogram, 134 MB volume)
-SMALL = dict(NA=360, NV=128, NH=512, PHANTOM=(344, 344, 128),
-             WORKLOAD="parallel-beam SIRT, 344x344x128 phantom, 360 angles, 512x128 detector, "
-                      "512x512x128 grid (profiling size)")
+# than L2: 189 MB sinogram, 268 MB volume)
+SMALL = dict(NA=360, NV=256, NH=512, PHANTOM=(344, 344, 256),
+             WORKLOAD="parallel-beam SIRT, 344x344x256 phantom, 360 angles, 512x256 detector, "
+                      "512x512x256 grid (profiling size)")
 
 
 def parse():

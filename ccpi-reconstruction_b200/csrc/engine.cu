@@ -191,7 +191,8 @@ int plan_create(const ccpi_geometry *gi, ccpi_plan **out) {
     g.vlo = upload(p, vlo);
     g.vhi = upload(p, vhi);
     ok = ok && g.yoff && g.ioff && g.blen && g.map && g.vlo && g.vhi;
-    p->fp_grid = int(std::min<i64>((i64(na) * nh + 3) / 4, 148 * 16));
+    p->fp_grid = pb_fp_ctas(g);
+    ok = ok && pb_prepare() == 0;
     p->bp_parts = pb_bp_tiles(g);
   } else {
     if (nv < 2) {
@@ -319,7 +320,7 @@ int plan_create(const ccpi_geometry *gi, ccpi_plan **out) {
 int forward(const ccpi_plan *p, const float *vol, float *pix, int mode, const Epi &e,
             cudaStream_t st) {
   if (p->g.kind == CCPI_PARALLEL)
-    return pb_forward(p->g, vol, pix, mode, e, p->fp_grid, st);
+    return pb_forward(p->g, vol, pix, mode, e, p->fp_grid, p->err, st);
   return cb_forward(p->g, vol, pix, mode, e, p->hrange, p->fp_grid, st);
 }
 
@@ -473,10 +474,11 @@ bool check_err(const ccpi_plan *p) {
   cudaMemcpy(&h, p->err, sizeof(int), cudaMemcpyDeviceToHost);
   if (h) {
     cudaMemset(p->err, 0, sizeof(int));
-    set_error(h == 1 ? "projector: more detector columns per voxel than the back "
-                       "projector stages (voxel much larger than a pixel)"
-                     : "projector: cone back projector ray list overflow (voxel "
-                       "shadow wider than 24 detector columns)");
+    set_error(h == 1   ? "projector: more detector columns per voxel than the back "
+                         "projector stages (voxel much larger than a pixel)"
+              : h == 2 ? "projector: cone back projector ray list overflow (voxel "
+                         "shadow wider than 24 detector columns)"
+                       : "projector: a ray crosses more than 256 xy blocks");
     return false;
   }
   return true;

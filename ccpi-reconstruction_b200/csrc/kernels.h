@@ -7,7 +7,9 @@ namespace ccpi {
 
 // projectors (pb_project.cu, cb_project.cu); out is overwritten
 int pb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
-               int grid, cudaStream_t st);
+               int grid, int *err, cudaStream_t st);
+int pb_prepare();
+int pb_fp_ctas(const Geom &g);
 int pb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
                 int *err, cudaStream_t st);
 int pb_bp_tiles(const Geom &g);

@@ -277,7 +277,7 @@ __device__ void store_partial(double ssq, const Epi &e) {
 // Staged cell lists: the warp-uniform walk emits (column, length) pairs into
 // the warp's slice of shared memory; the lanes then accumulate them in
 // order, four cells at a time with all loads issued before the adds.
-constexpr int kFpWarps = 4;
+constexpr int kFpWarps = 8;  // warps of a CTA trace one detector column at 8 angles
 constexpr int kListCap = 256; // staged cells per warp
 constexpr int kBlockCells = 72; // most cells one ray has in one 32x32 block
 
@@ -286,15 +286,87 @@ struct Cell {
   float len;
 };
 
-// ---- forward, float4 rows (row v -> slice v, nv and nz multiples of 4)
+// ---- forward, lane-parallel walk (row v -> slice v, nv and nz multiples of 4)
+//
+// One warp per ray.  The ray's blocks are first enumerated in the
+// reference's order (lanes over block columns, prefix sum for positions).
+// Then, 16 blocks at a time, every lane of a half-warp walks one block into its own slot of
+// shared memory (struct-of-arrays, odd stride: conflict-free), and the warp
+// replays the slots in block order with its lanes over detector rows.  The
+// per-row additions are the same, in the same order, as the warp-uniform
+// walk above; only who evaluates the walk changes, so the instruction cost
+// of the FP64 walk is shared by 32 blocks.
+constexpr int kLaneWarps = 4;
+constexpr int kWalkLanes = 16;  // blocks walked in parallel per round
+constexpr int kSlotCap = 73;    // cells of one ray in one block (<= 66), odd stride
+constexpr int kMaxBlocks = 256; // blocks one ray may visit (nbx + nby bound)
+
+struct LaneSmem {
+  int col[kWalkLanes * kSlotCap];
+  float len[kWalkLanes * kSlotCap];
+  int blk[kMaxBlocks];
+};
+
+// Blocks of ray (c, s, p2) passing the reference's tests, counted (emit ==
+// nullptr) or written in y-block order for one block column.
+__device__ __forceinline__ int pb_column_blocks(const Geom &g, int h, double c, double s,
+                                                double p2x, double p2y, bool par_y, bool par_x,
+                                                int bxi, int *emit, int pos) {
+  const double dx = g.size[0], dy = g.size[1];
+  const int nby = (g.ny + kBlock - 1) / kBlock;
+  const int bx0 = bxi * kBlock, nxb = min(kBlock, g.nx - bx0);
+  const double vx = g.origin[0] + double(bx0) * dx;
+  const double wx = g.origin[0] + double(bx0 + nxb) * dx;
+  int lo = 0, hi = nby - 1;
+  if (par_y) {
+    const int ix = int(floor((p2x - vx) / dx));
+    if (ix < 0 || ix >= nxb)
+      return 0;
+  } else if (!par_x) {
+    const double tt = s / c;
+    const double ya = p2y + (vx - p2x) * tt, yb = p2y + (wx - p2x) * tt;
+    const double margin = 1e-3 * dy;
+    const double ylo = fmin(ya, yb) - margin, yhi = fmax(ya, yb) + margin;
+    const double bsz = double(kBlock) * dy;
+    const double flo = floor((ylo - g.origin[1]) / bsz);
+    const double fhi = floor((yhi - g.origin[1]) / bsz);
+    if (fhi < 0.0 || flo > double(nby - 1))
+      return 0;
+    lo = flo < 0.0 ? 0 : int(flo);
+    hi = fhi > double(nby - 1) ? nby - 1 : int(fhi);
+  }
+  int cnt = 0;
+  for (int byi = lo; byi <= hi; byi++) {
+    const int by0 = byi * kBlock, nyb = min(kBlock, g.ny - by0);
+    const double vy = g.origin[1] + double(by0) * dy;
+    const double wy = g.origin[1] + double(by0 + nyb) * dy;
+    int hmin, hmax;
+    pb_hrange(g, vx, wx, vy, wy, c, s, hmin, hmax);
+    if (h < hmin || h > hmax)
+      continue;
+    if (par_x) {
+      const int jy = int(floor((p2y - vy) / dy));
+      if (jy < 0 || jy >= nyb)
+        continue;
+    }
+    if (emit && pos + cnt < kMaxBlocks)
+      emit[pos + cnt] = (bxi << 16) | byi;
+    cnt++;
+  }
+  return cnt;
+}
+
 template <int NQ, int EPI>
-__global__ void __launch_bounds__(kFpWarps * 32) pb_fp_vec4(Geom g, const float *__restrict__ vol,
-                                                            float *__restrict__ pix, Epi e, int v0) {
-  __shared__ Cell lists[kFpWarps][kListCap];
+__global__ void __launch_bounds__(kLaneWarps * 32)
+    pb_fp_lanes(Geom g, const float *__restrict__ vol, float *__restrict__ pix, Epi e, int v0,
+                int *err) {
+  extern __shared__ unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  Cell *L = lists[wib];
-  const int nwarps_total = gridDim.x * kFpWarps;
-  const int nrays = g.na * g.nh;
+  LaneSmem &S = reinterpret_cast<LaneSmem *>(smem_raw)[wib];
+  const double eps = double(kEps);
+  const double dx = g.size[0], dy = g.size[1];
+  const int nbx = (g.nx + kBlock - 1) / kBlock;
+  const int ncol = g.nx * g.ny;
   bool vok[NQ];
   int vq[NQ];
 #pragma unroll
@@ -303,60 +375,186 @@ __global__ void __launch_bounds__(kFpWarps * 32) pb_fp_vec4(Geom g, const float 
     vok[q] = vq[q] < g.nv;
   }
   double ssq = 0.0;
-  for (int ray = blockIdx.x * kFpWarps + wib; ray < nrays; ray += nwarps_total) {
-    const int a = ray / g.nh, h = ray - a * g.nh;
+  const int nat = (g.na + kLaneWarps - 1) / kLaneWarps;
+  const int ntiles = nat * g.nh;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int h = t / nat;
+    const int a = (t - h * nat) * kLaneWarps + wib;
+    if (a >= g.na)
+      continue;
+    const int ray = a * g.nh + h;
+    const double c = g.cosA[a], s = g.sinA[a], hv = g.hpix[h];
+    const double p2x = c * g.det_x - s * hv;
+    const double p2y = s * g.det_x + c * hv;
+    const bool par_y = fabs(c) < eps, par_x = !par_y && fabs(s) < eps;
     float4 acc[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++)
       acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-    int n = 0;
-    auto flush = [&]() {
-      __syncwarp();
-      int m = 0;
-      for (; m + 4 <= n; m += 4) {
-        Cell c4[4];
-        float4 x[4][NQ];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          c4[j] = L[m + j];
-#pragma unroll
-          for (int q = 0; q < NQ; q++)
-            x[j][q] = (c4[j].col >= 0 && vok[q])
-                          ? __ldg(reinterpret_cast<const float4 *>(vol + i64(c4[j].col) * g.nz + vq[q]))
-                          : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!(par_y && fabs(s) < eps)) {
+      // ---- enumerate the blocks: x-block major, y-block ascending
+      int nblk = 0;
+      for (int bbase = 0; bbase < nbx; bbase += 32) {
+        const int bxi = bbase + lane;
+        const int cnt =
+            bxi < nbx ? pb_column_blocks(g, h, c, s, p2x, p2y, par_y, par_x, bxi, nullptr, 0) : 0;
+        int incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o)
+            incl += y;
         }
+        if (cnt)
+          pb_column_blocks(g, h, c, s, p2x, p2y, par_y, par_x, bxi, S.blk, nblk + incl - cnt);
+        nblk += __shfl_sync(0xffffffffu, incl, 31);
+      }
+      if (nblk > kMaxBlocks) {
+        if (lane == 0)
+          atomicExch(err, 3);
+        nblk = kMaxBlocks;
+      }
+      __syncwarp();
+      const double ic = par_y ? 0.0 : 1.0 / c, is = par_x ? 0.0 : 1.0 / s;
+      const int sx = c > 0.0 ? 1 : -1, sy = s > 0.0 ? 1 : -1;
+      const int ox = sx > 0 ? 1 : 0, oy = sy > 0 ? 1 : 0;
+      const bool x_face_first = !(sx > 0 && sy < 0);
+      // ---- walk kWalkLanes blocks at a time, one per lane
+      for (int r0 = 0; r0 < nblk; r0 += kWalkLanes) {
+        const int j = r0 + lane;
+        int n = 0;
+        int *mycol = S.col + (lane % kWalkLanes) * kSlotCap;
+        float *mylen = S.len + (lane % kWalkLanes) * kSlotCap;
+        if (lane < kWalkLanes && j < nblk) {
+          const int id = S.blk[j];
+          const int bxi = id >> 16, byi = id & 0xffff;
+          const int bx0 = bxi * kBlock, nxb = min(kBlock, g.nx - bx0);
+          const int by0 = byi * kBlock, nyb = min(kBlock, g.ny - by0);
+          const double vx = g.origin[0] + double(bx0) * dx;
+          const double vy = g.origin[1] + double(by0) * dy;
+          if (par_y) {
+            const int ix = int(floor((p2x - vx) / dx));
+            const float len = float(dy);
+            for (int tt = 0; tt < nyb; tt++) {
+              const int jj = s < 0.0 ? nyb - 1 - tt : tt;
+              const int col = (bx0 + ix) * g.ny + by0 + jj;
+              mycol[n] = unsigned(col) < unsigned(ncol) ? col : -1;
+              mylen[n] = len;
+              n++;
+            }
+          } else if (par_x) {
+            const int jy = int(floor((p2y - vy) / dy));
+            const float len = float(dx);
+            for (int tt = 0; tt < nxb; tt++) {
+              const int ii = c < 0.0 ? nxb - 1 - tt : tt;
+              const int col = (bx0 + ii) * g.ny + by0 + jy;
+              mycol[n] = unsigned(col) < unsigned(ncol) ? col : -1;
+              mylen[n] = len;
+              n++;
+            }
+          } else {
+            const double xn = vx + double(nxb) * dx, yn = vy + double(nyb) * dy;
+            const double ax0 = (vx - p2x) * ic, ay0 = (vy - p2y) * is;
+            const double axn = (xn - p2x) * ic, ayn = (yn - p2y) * is;
+            const double amin =
+                dmax(dmax(dmin(ax0, axn), dmin(ay0, ayn)), double(-g.d_conv));
+            const double amax = dmin(dmin(dmax(ax0, axn), dmax(ay0, ayn)), 0.0);
+            if (amin < amax - eps) {
+              int x = 0, y = 0;
+              const double axe = sx > 0 ? ax0 : axn, aye = sy > 0 ? ay0 : ayn;
+              if (x_face_first) {
+                if (amin == axe) {
+                  x = sx > 0 ? 0 : nxb - 1;
+                  y = (sx < 0 && sy < 0 && amin == ayn)
+                          ? nyb - 1
+                          : int(floor((p2y + amin * s - vy) / dy));
+                } else if (amin == aye) {
+                  x = int(floor((p2x + amin * c - vx) / dx));
+                  y = sy > 0 ? 0 : nyb - 1;
+                }
+              } else {
+                if (amin == aye) {
+                  x = int(floor((p2x + amin * c - vx) / dx));
+                  y = nyb - 1;
+                } else if (amin == axe) {
+                  x = 0;
+                  y = int(floor((p2y + amin * s - vy) / dy));
+                }
+              }
+              double nxa = (vx + double(x + ox) * dx - p2x) * ic;
+              double nya = (vy + double(y + oy) * dy - p2y) * is;
+              double ap = amin;
+              int col = (bx0 + x) * g.ny + (by0 + y);
+              const int cstep_x = sx * g.ny;
+              while ((sx > 0 ? x < nxb : x >= 0) && (sy > 0 ? y < nyb : y >= 0) &&
+                     n < kSlotCap) {
+                const bool tx = nxa < nya - eps;
+                const bool ty = !tx && (nya < nxa - eps);
+                const bool both = !tx && !ty;
+                const double nxt = tx ? nxa : (ty ? nya : dmax(nxa, nya));
+                mycol[n] = unsigned(col) < unsigned(ncol) ? col : -1;
+                mylen[n] = float(nxt - ap);
+                n++;
+                ap = nxt;
+                if (tx || both) {
+                  x += sx;
+                  col += cstep_x;
+                  nxa = (vx + double(x + ox) * dx - p2x) * ic;
+                }
+                if (ty || both) {
+                  y += sy;
+                  col += sy;
+                  nya = (vy + double(y + oy) * dy - p2y) * is;
+                }
+              }
+            }
+          }
+        }
+        __syncwarp();
+        // ---- replay the slots in block order, lanes over rows
+        const int nr = min(kWalkLanes, nblk - r0);
+        for (int jj = 0; jj < nr; jj++) {
+          const int nj = __shfl_sync(0xffffffffu, n, jj);
+          const int *cc = S.col + jj * kSlotCap;
+          const float *ll = S.len + jj * kSlotCap;
+          int m = 0;
+          for (; m + 4 <= nj; m += 4) {
+            int c4[4];
+            float l4[4];
+            float4 xv[4][NQ];
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-          if (c4[j].col >= 0) {
+            for (int u = 0; u < 4; u++) {
+              c4[u] = cc[m + u];
+              l4[u] = ll[m + u];
+#pragma unroll
+              for (int q = 0; q < NQ; q++)
+                xv[u][q] = (c4[u] >= 0 && vok[q])
+                               ? __ldg(reinterpret_cast<const float4 *>(vol + i64(c4[u]) * g.nz +
+                                                                        vq[q]))
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+              if (c4[u] >= 0) {
+#pragma unroll
+                for (int q = 0; q < NQ; q++)
+                  axpy4(acc[q], xv[u][q], l4[u]);
+              }
+          }
+          for (; m < nj; m++) {
+            const int c1 = cc[m];
+            if (c1 < 0)
+              continue;
+            const float l1 = ll[m];
 #pragma unroll
             for (int q = 0; q < NQ; q++)
-              axpy4(acc[q], x[j][q], c4[j].len);
+              if (vok[q])
+                axpy4(acc[q],
+                      __ldg(reinterpret_cast<const float4 *>(vol + i64(c1) * g.nz + vq[q])), l1);
           }
+        }
+        __syncwarp();
       }
-      for (; m < n; m++) {
-        const Cell c1 = L[m];
-        if (c1.col < 0)
-          continue;
-#pragma unroll
-        for (int q = 0; q < NQ; q++)
-          if (vok[q])
-            axpy4(acc[q], __ldg(reinterpret_cast<const float4 *>(vol + i64(c1.col) * g.nz + vq[q])),
-                  c1.len);
-      }
-      __syncwarp();
-      n = 0;
-    };
-    auto emit = [&](int col, float len) {
-      if (lane == 0)
-        L[n] = Cell{col, len};
-      n++;
-    };
-    auto room = [&]() {
-      if (n > kListCap - kBlockCells)
-        flush();
-    };
-    pb_trace_ray(g, a, h, emit, room);
-    flush();
+    }
     const i64 rbase = i64(ray) * g.nv;
 #pragma unroll
     for (int q = 0; q < NQ; q++) {
@@ -372,7 +570,7 @@ __global__ void __launch_bounds__(kFpWarps * 32) pb_fp_vec4(Geom g, const float 
     }
   }
   if (EPI == EPI_NORM)
-    store_partial<kFpWarps>(ssq, e);
+    store_partial<kLaneWarps>(ssq, e);
 }
 
 // ---- forward, any row->slice mapping (p2D.cpp:63-213 cases 2, 4, default)
@@ -382,8 +580,6 @@ __global__ void __launch_bounds__(kFpWarps * 32) pb_fp_scalar(Geom g, const floa
   __shared__ Cell lists[kFpWarps][kListCap];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   Cell *L = lists[wib];
-  const int nwarps_total = gridDim.x * kFpWarps;
-  const int nrays = g.na * g.nh;
   double ssq = 0.0;
   int zmap[NS];
 #pragma unroll
@@ -393,8 +589,14 @@ __global__ void __launch_bounds__(kFpWarps * 32) pb_fp_scalar(Geom g, const floa
     if (zmap[q] >= g.nz)
       zmap[q] = -1; // the reference reads past the column here
   }
-  for (int ray = blockIdx.x * kFpWarps + wib; ray < nrays; ray += nwarps_total) {
-    const int a = ray / g.nh, h = ray - a * g.nh;
+  const int nat = (g.na + kFpWarps - 1) / kFpWarps;
+  const int ntiles = nat * g.nh;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int h = t / nat;
+    const int a = (t - h * nat) * kFpWarps + wib;
+    if (a >= g.na)
+      continue;
+    const int ray = a * g.nh + h;
     float acc[NS];
 #pragma unroll
     for (int q = 0; q < NS; q++)
@@ -719,18 +921,16 @@ __global__ void __launch_bounds__(256) pb_bp_scalar(Geom g, const float *__restr
 }
 
 template <int EPI>
-int launch_fp(const Geom &g, const float *vol, float *pix, const Epi &e, int grid,
+int launch_fp(const Geom &g, const float *vol, float *pix, const Epi &e, int grid, int *err,
               cudaStream_t st) {
   const bool vec4 = g.map_type == 1 && (g.nv % 4) == 0 && (g.nz % 4) == 0;
   if (vec4) {
-    for (int v0 = 0; v0 < g.nv; v0 += 512) {
-      const int left = g.nv - v0;
-      if (left > 256)
-        pb_fp_vec4<4, EPI><<<grid, kFpWarps * 32, 0, st>>>(g, vol, pix, e, v0);
-      else if (left > 128)
-        pb_fp_vec4<2, EPI><<<grid, kFpWarps * 32, 0, st>>>(g, vol, pix, e, v0);
+    const size_t smem = sizeof(LaneSmem) * kLaneWarps;
+    for (int v0 = 0; v0 < g.nv; v0 += 256) {
+      if (g.nv - v0 > 128)
+        pb_fp_lanes<2, EPI><<<grid, kLaneWarps * 32, smem, st>>>(g, vol, pix, e, v0, err);
       else
-        pb_fp_vec4<1, EPI><<<grid, kFpWarps * 32, 0, st>>>(g, vol, pix, e, v0);
+        pb_fp_lanes<1, EPI><<<grid, kLaneWarps * 32, smem, st>>>(g, vol, pix, e, v0, err);
     }
   } else {
     for (int v0 = 0; v0 < g.nv; v0 += 256) {
@@ -815,18 +1015,37 @@ int launch_bp(const Geom &g, const float *pix, float *vol, const Epi &e, int *er
 } // namespace
 
 int pb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
-               int grid, cudaStream_t st) {
+               int grid, int *err, cudaStream_t st) {
   switch (mode) {
   case EPI_STORE:
-    return launch_fp<EPI_STORE>(g, vol, pix, e, grid, st);
+    return launch_fp<EPI_STORE>(g, vol, pix, e, grid, err, st);
   case EPI_NORM:
-    return launch_fp<EPI_NORM>(g, vol, pix, e, grid, st);
+    return launch_fp<EPI_NORM>(g, vol, pix, e, grid, err, st);
   case EPI_SIRT:
-    return launch_fp<EPI_SIRT>(g, vol, pix, e, grid, st);
+    return launch_fp<EPI_SIRT>(g, vol, pix, e, grid, err, st);
   case EPI_MLEM:
-    return launch_fp<EPI_MLEM>(g, vol, pix, e, grid, st);
+    return launch_fp<EPI_MLEM>(g, vol, pix, e, grid, err, st);
   }
   return 1;
+}
+
+// Opt the forward kernels into their shared memory (done once, outside any
+// graph capture).
+int pb_prepare() {
+  const int smem = int(sizeof(LaneSmem) * kLaneWarps);
+  const void *fns[] = {(const void *)pb_fp_lanes<1, EPI_STORE>, (const void *)pb_fp_lanes<2, EPI_STORE>,
+                       (const void *)pb_fp_lanes<1, EPI_NORM>,  (const void *)pb_fp_lanes<2, EPI_NORM>,
+                       (const void *)pb_fp_lanes<1, EPI_SIRT>,  (const void *)pb_fp_lanes<2, EPI_SIRT>,
+                       (const void *)pb_fp_lanes<1, EPI_MLEM>,  (const void *)pb_fp_lanes<2, EPI_MLEM>};
+  for (const void *f : fns)
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+      return 1;
+  return 0;
+}
+
+int pb_fp_ctas(const Geom &g) {
+  const long long tiles = (long long)((g.na + kLaneWarps - 1) / kLaneWarps) * g.nh;
+  return int(tiles < 148 * 5 ? tiles : 148 * 5);
 }
 
 int pb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
