@@ -24,6 +24,8 @@ per-iteration |A^T r| instead.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from .. import _native as N
@@ -31,7 +33,8 @@ from .. import _native as N
 __all__ = ["cgls", "cgls_conv", "sirt", "mlem", "cgls_tikhonov", "cgls_TVreg",
            "cgls_step", "cgls_conv_step", "sirt_step", "mlem_step", "cgls_tikhonov_step",
            "cgls_TVreg_step", "pb_forward_project", "pb_backward_project",
-           "pb_setup_geometry_from_image", "pb_setup_geometry_from_acquisition", "grid"]
+           "pb_setup_geometry_from_image", "pb_setup_geometry_from_acquisition", "grid",
+           "reconstruct_batched"]
 
 
 def grid(n_angles, n_v, n_h, rotation_centre, resolution):
@@ -111,6 +114,54 @@ def cgls_TVreg(pixels, angles, rotation_centre, resolution, niterations, nthread
                norm_r, is_pixels_in_log, real_norms=False):
     return _reconstruct(N.CGLS_TV, pixels, angles, rotation_centre, resolution, niterations,
                         nthreads, is_pixels_in_log, regularize, norm_r, real_norms=real_norms)
+
+
+_ALGS = {"cgls": N.CGLS, "sirt": N.SIRT, "mlem": N.MLEM, "cgls_tikhonov": N.CGLS_TIKHONOV,
+         "cgls_TVreg": N.CGLS_TV}
+
+
+def reconstruct_batched(algorithm, pixels, angles, rotation_centre, resolution, niterations,
+                        nthreads, is_pixels_in_log, regularize=None):
+    """Many independent problems of uneven sizes in one go (no reference
+    counterpart; each result equals the single call ``algorithm(pixels[i],
+    angles[i], rotation_centre[i], resolution, niterations, nthreads,
+    [regularize[i], zeros,] is_pixels_in_log)``).
+
+    algorithm: "cgls", "sirt", "mlem", "cgls_tikhonov" or "cgls_TVreg";
+    pixels / angles: sequences of (n_angles, n_v, n_h) arrays and angle
+    lists; rotation_centre: a number or one per problem; regularize: one
+    weight per problem for the regularised solvers.  Returns the list of
+    volumes.  Every problem's kernels go into one CUDA graph per iteration.
+    """
+    del nthreads
+    if algorithm not in _ALGS:
+        raise ValueError(f"unknown algorithm {algorithm!r}")
+    n = len(pixels)
+    if len(angles) != n:
+        raise ValueError("pixels and angles must have the same length")
+    pix = [N.f32(p, "pixels", 3) for p in pixels]
+    ang = [N.f32(a, "angles", 1) for a in angles]
+    cor = np.broadcast_to(np.asarray(rotation_centre, np.float64), (n,)).copy()
+    na = np.array([p.shape[0] for p in pix], np.int32)
+    nv = np.array([p.shape[1] for p in pix], np.int32)
+    nh = np.array([p.shape[2] for p in pix], np.int32)
+    for i in range(n):
+        if ang[i].shape[0] != na[i]:
+            raise ValueError(f"problem {i}: number of projections ({na[i]}) doesn't match "
+                             f"angle array ({ang[i].shape[0]})")
+    reg = None
+    if regularize is not None:
+        reg = np.broadcast_to(np.asarray(regularize, np.float64), (n,)).copy()
+    outs = []
+    for i in range(n):
+        gx, gy, gz, _, _ = grid(na[i], nv[i], nh[i], cor[i], resolution)
+        outs.append(np.zeros((gx, gy, gz), np.float32))
+    ptrs = lambda arrs: (ctypes.c_void_p * n)(*[a.ctypes.data for a in arrs])  # noqa: E731
+    N.check(N.lib.ccpi_pb_reconstruct_batched(
+        n, _ALGS[algorithm], ptrs(pix), na, nv, nh, ptrs(ang), cor, int(resolution),
+        int(niterations), int(bool(is_pixels_in_log)),
+        reg.ctypes.data if reg is not None else None, ptrs(outs)), "batched reconstruction")
+    return outs
 
 
 # ---- warm-start forms (diamond_wrapper.cpp:140-411): the previous volume

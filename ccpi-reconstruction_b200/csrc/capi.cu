@@ -408,6 +408,72 @@ int ccpi_pb_reconstruct(int alg, const float *pixels, int na, int nv, int nh,
   return solve_on_host_data(G, alg, src, true, na, nv, nh, x0, niter, lambda, norms, volume);
 }
 
+int ccpi_pb_reconstruct_batched(int n, int alg, const float *const *pixels, const int *na,
+                                const int *nv, const int *nh, const float *const *angles_deg,
+                                const double *cor, int ppv, int niter, int is_log,
+                                const double *lambda, float *const *volumes) {
+  ccpi::g_last_error.clear();
+  if (n < 0 || (n > 0 && (!pixels || !na || !nv || !nh || !angles_deg || !cor || !volumes))) {
+    set_error("ccpi_pb_reconstruct_batched: bad arguments");
+    return 1;
+  }
+  if (n == 0)
+    return 0;
+  std::vector<HostGeometry> G(n);
+  std::vector<PlanHolder> P(n);
+  std::vector<i64> off_raw(n + 1, 0), off_sino(n + 1, 0), off_x(n + 1, 0);
+  for (int i = 0; i < n; i++) {
+    if (!pixels[i] || !angles_deg[i] || !volumes[i]) {
+      set_error("ccpi_pb_reconstruct_batched: null buffer for problem " + std::to_string(i));
+      return 1;
+    }
+    if (!pb_geometry(na[i], nv[i], nh[i], cor[i], ppv, angles_deg[i], G[i]))
+      return 1;
+    if (ccpi::plan_create(&G[i].g, &P[i].p))
+      return 2;
+    // 16-byte aligned sub-buffers
+    auto up4 = [](i64 x) { return (x + 3) & ~i64(3); };
+    off_raw[i + 1] = off_raw[i] + up4(i64(na[i]) * nv[i] * nh[i]);
+    off_sino[i + 1] = off_sino[i] + up4(P[i].p->npix);
+    off_x[i + 1] = off_x[i] + up4(P[i].p->nvox);
+  }
+  DevBuf draw, dsino, dx;
+  if (!draw.alloc(off_raw[n] * 4) || !dsino.alloc(off_sino[n] * 4) || !dx.alloc(off_x[n] * 4))
+    return 2;
+  cudaStream_t st = 0;
+  std::vector<float> logged;
+  std::vector<const float *> ds(n);
+  std::vector<float *> dv(n);
+  std::vector<const ccpi_plan *> pl(n);
+  for (int i = 0; i < n; i++) {
+    const i64 raw = i64(na[i]) * nv[i] * nh[i];
+    const float *src = pixels[i];
+    if (!is_log) {
+      logged.resize(size_t(raw));
+      neglog_host(pixels[i], logged.data(), raw);
+      src = logged.data();
+    }
+    float *r = draw.f() + off_raw[i];
+    // synchronous copy: `logged` is reused by the next problem
+    if (!ccpi::cuda_ok(cudaMemcpy(r, src, raw * 4, cudaMemcpyHostToDevice), "upload sinogram"))
+      return 2;
+    float *s = dsino.f() + off_sino[i];
+    ccpi::k_pack_parallel(r, s, na[i], nv[i], nh[i], G[i].nv_pad, G[i].v_offset, st);
+    ds[i] = s;
+    dv[i] = dx.f() + off_x[i];
+    pl[i] = P[i].p;
+  }
+  cudaMemsetAsync(dx.p, 0, off_x[n] * 4, st);
+  const int rc = ccpi::solve_batched(n, pl.data(), alg, ds.data(), dv.data(), niter, lambda, st);
+  if (rc)
+    return rc;
+  for (int i = 0; i < n; i++)
+    if (!ccpi::cuda_ok(cudaMemcpy(volumes[i], dv[i], P[i].p->nvox * 4, cudaMemcpyDeviceToHost),
+                       "download volume"))
+      return 2;
+  return 0;
+}
+
 int ccpi_pb_forward_project(const float *volume, int vx, int vy, int vz, const float *angles_deg,
                             int na, int ppv, float *out, int out_dims[3]) {
   ccpi::g_last_error.clear();

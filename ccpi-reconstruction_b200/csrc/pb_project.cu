@@ -296,8 +296,18 @@ struct Cell {
 // per-row additions are the same, in the same order, as the warp-uniform
 // walk above; only who evaluates the walk changes, so the instruction cost
 // of the FP64 walk is shared by 32 blocks.
+#ifndef PB_WALK_LANES
+#define PB_WALK_LANES 16
+#endif
+#ifndef PB_FP_CTAS_PER_SM
+#define PB_FP_CTAS_PER_SM 4
+#endif
 constexpr int kLaneWarps = 4;
-constexpr int kWalkLanes = 16;  // blocks walked in parallel per round
+#ifndef PB_FP_UNROLL
+#define PB_FP_UNROLL 4
+#endif
+constexpr int kWalkLanes = PB_WALK_LANES; // blocks walked in parallel per round
+constexpr int kReplayUnroll = PB_FP_UNROLL; // cells whose loads are in flight together
 constexpr int kSlotCap = 73;    // cells of one ray in one block (<= 66), odd stride
 constexpr int kMaxBlocks = 256; // blocks one ray may visit (nbx + nby bound)
 
@@ -356,8 +366,11 @@ __device__ __forceinline__ int pb_column_blocks(const Geom &g, int h, double c, 
   return cnt;
 }
 
+#ifndef PB_FP_MINB
+#define PB_FP_MINB 1
+#endif
 template <int NQ, int EPI>
-__global__ void __launch_bounds__(kLaneWarps * 32)
+__global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
     pb_fp_lanes(Geom g, const float *__restrict__ vol, float *__restrict__ pix, Epi e, int v0,
                 int *err) {
   extern __shared__ unsigned char smem_raw[];
@@ -517,12 +530,12 @@ __global__ void __launch_bounds__(kLaneWarps * 32)
           const int *cc = S.col + jj * kSlotCap;
           const float *ll = S.len + jj * kSlotCap;
           int m = 0;
-          for (; m + 4 <= nj; m += 4) {
-            int c4[4];
-            float l4[4];
-            float4 xv[4][NQ];
+          for (; m + kReplayUnroll <= nj; m += kReplayUnroll) {
+            int c4[kReplayUnroll];
+            float l4[kReplayUnroll];
+            float4 xv[kReplayUnroll][NQ];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < kReplayUnroll; u++) {
               c4[u] = cc[m + u];
               l4[u] = ll[m + u];
 #pragma unroll
@@ -533,7 +546,7 @@ __global__ void __launch_bounds__(kLaneWarps * 32)
                                : make_float4(0.f, 0.f, 0.f, 0.f);
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++)
+            for (int u = 0; u < kReplayUnroll; u++)
               if (c4[u] >= 0) {
 #pragma unroll
                 for (int q = 0; q < NQ; q++)
@@ -1045,7 +1058,7 @@ int pb_prepare() {
 
 int pb_fp_ctas(const Geom &g) {
   const long long tiles = (long long)((g.na + kLaneWarps - 1) / kLaneWarps) * g.nh;
-  return int(tiles < 148 * 5 ? tiles : 148 * 5);
+  return int(tiles < 148 * PB_FP_CTAS_PER_SM ? tiles : 148 * PB_FP_CTAS_PER_SM);
 }
 
 int pb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,

@@ -90,6 +90,23 @@ int ccpi_pb_reconstruct(int alg, const float *pixels, int n_angles, int n_v,
                         double regularize, const float *x0, double *norms,
                         float *volume);
 
+/* n independent ccpi_pb_reconstruct problems of uneven sizes solved
+ * together: one CUDA graph per iteration holds every problem's kernels.
+ * The reference has no batched call; each problem i gives the same volume
+ * as ccpi_pb_reconstruct(alg, pixels[i], na[i], nv[i], nh[i],
+ * angles_deg[i], cor[i], pixels_per_voxel, niterations, -, is_log,
+ * regularize[i], NULL, NULL, volumes[i]) (reconstruct_iter,
+ * Wrappers/Python/src/diamond_wrapper.cpp:53-137, called n times).
+ * regularize: NULL (all 0) or n weights; volumes[i]: ccpi_pb_grid's
+ * nx*ny*nz floats for problem i. */
+int ccpi_pb_reconstruct_batched(int n, int alg, const float *const *pixels,
+                                const int *n_angles, const int *n_v,
+                                const int *n_h, const float *const *angles_deg,
+                                const double *rotation_centre,
+                                int pixels_per_voxel, int niterations,
+                                int is_pixels_in_log, const double *regularize,
+                                float *const *volumes);
+
 /* parallelbeam.alg.pb_forward_project (diamond_wrapper.cpp:421-556):
  * volume (vx, vy, vz) -> (n_angles, n_v_padded, max(vx, vy)).  With
  * out == NULL only out_dims is filled. */
