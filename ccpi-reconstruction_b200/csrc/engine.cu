@@ -478,7 +478,8 @@ bool check_err(const ccpi_plan *p) {
                          "projector stages (voxel much larger than a pixel)"
               : h == 2 ? "projector: cone back projector ray list overflow (voxel "
                          "shadow wider than 24 detector columns)"
-                       : "projector: a ray crosses more than 256 xy blocks");
+                       : "projector: a ray's staged xy blocks or cells overflowed the "
+                         "forward projector's shared-memory staging");
     return false;
   }
   return true;

@@ -290,30 +290,30 @@ struct Cell {
 //
 // One warp per ray.  The ray's blocks are first enumerated in the
 // reference's order (lanes over block columns, prefix sum for positions).
-// Then, 16 blocks at a time, every lane of a half-warp walks one block into its own slot of
-// shared memory (struct-of-arrays, odd stride: conflict-free), and the warp
-// replays the slots in block order with its lanes over detector rows.  The
-// per-row additions are the same, in the same order, as the warp-uniform
-// walk above; only who evaluates the walk changes, so the instruction cost
-// of the FP64 walk is shared by 32 blocks.
+// Then, 16 blocks at a time, every lane of a half-warp walks one block into
+// its own slot of shared memory, and the warp replays the slots in block
+// order with its lanes over detector rows, reading two staged cells per
+// 16-byte shared load (all lanes read the same cells: broadcast).  The
+// per-row additions are the same, in the same order, as a one-ray-at-a-time
+// walk; only who evaluates the walk changes, so the instruction cost of the
+// FP64 walk is shared by 16 blocks.
 #ifndef PB_WALK_LANES
 #define PB_WALK_LANES 16
 #endif
 #ifndef PB_FP_CTAS_PER_SM
-#define PB_FP_CTAS_PER_SM 4
+#define PB_FP_CTAS_PER_SM 5
 #endif
 constexpr int kLaneWarps = 4;
-#ifndef PB_FP_UNROLL
-#define PB_FP_UNROLL 4
-#endif
 constexpr int kWalkLanes = PB_WALK_LANES; // blocks walked in parallel per round
-constexpr int kReplayUnroll = PB_FP_UNROLL; // cells whose loads are in flight together
-constexpr int kSlotCap = 73;    // cells of one ray in one block (<= 66), odd stride
-constexpr int kMaxBlocks = 256; // blocks one ray may visit (nbx + nby bound)
+constexpr int kSlotCap = 66;    // cells of one ray in one block (<= 65); even, so
+                                // every other entry starts a 16-byte pair
+constexpr int kMaxBlocks = 192; // blocks one ray may visit (about nbx + nby)
 
+// One staged cell: .x = the column's offset in float4 units (column * nz / 4),
+// .y = the bits of its float length.  Cells outside the volume are dropped
+// when staged (they add nothing).
 struct LaneSmem {
-  int col[kWalkLanes * kSlotCap];
-  float len[kWalkLanes * kSlotCap];
+  uint2 cell[kWalkLanes * kSlotCap];
   int blk[kMaxBlocks];
 };
 
@@ -367,7 +367,10 @@ __device__ __forceinline__ int pb_column_blocks(const Geom &g, int h, double c, 
 }
 
 #ifndef PB_FP_MINB
-#define PB_FP_MINB 1
+#define PB_FP_MINB 5
+#endif
+#ifndef PB_FP_BATCH
+#define PB_FP_BATCH 4 // staged cells whose loads are issued together (4 or 2)
 #endif
 template <int NQ, int EPI>
 __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
@@ -380,6 +383,9 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
   const double dx = g.size[0], dy = g.size[1];
   const int nbx = (g.nx + kBlock - 1) / kBlock;
   const int ncol = g.nx * g.ny;
+  const unsigned nz4 = unsigned(g.nz) >> 2;
+  // this lane's rows v0 + q*128 + 4*lane .. +3 of column 0, as float4
+  const float4 *vb = reinterpret_cast<const float4 *>(vol) + (v0 >> 2) + lane;
   bool vok[NQ];
   int vq[NQ];
 #pragma unroll
@@ -435,8 +441,11 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
       for (int r0 = 0; r0 < nblk; r0 += kWalkLanes) {
         const int j = r0 + lane;
         int n = 0;
-        int *mycol = S.col + (lane % kWalkLanes) * kSlotCap;
-        float *mylen = S.len + (lane % kWalkLanes) * kSlotCap;
+        uint2 *myc = S.cell + (lane % kWalkLanes) * kSlotCap;
+        auto put = [&](int col, float len) {
+          if (unsigned(col) < unsigned(ncol))
+            myc[n++] = make_uint2(unsigned(col) * nz4, __float_as_uint(len));
+        };
         if (lane < kWalkLanes && j < nblk) {
           const int id = S.blk[j];
           const int bxi = id >> 16, byi = id & 0xffff;
@@ -449,20 +458,14 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
             const float len = float(dy);
             for (int tt = 0; tt < nyb; tt++) {
               const int jj = s < 0.0 ? nyb - 1 - tt : tt;
-              const int col = (bx0 + ix) * g.ny + by0 + jj;
-              mycol[n] = unsigned(col) < unsigned(ncol) ? col : -1;
-              mylen[n] = len;
-              n++;
+              put((bx0 + ix) * g.ny + by0 + jj, len);
             }
           } else if (par_x) {
             const int jy = int(floor((p2y - vy) / dy));
             const float len = float(dx);
             for (int tt = 0; tt < nxb; tt++) {
               const int ii = c < 0.0 ? nxb - 1 - tt : tt;
-              const int col = (bx0 + ii) * g.ny + by0 + jy;
-              mycol[n] = unsigned(col) < unsigned(ncol) ? col : -1;
-              mylen[n] = len;
-              n++;
+              put((bx0 + ii) * g.ny + by0 + jy, len);
             }
           } else {
             const double xn = vx + double(nxb) * dx, yn = vy + double(nyb) * dy;
@@ -504,9 +507,7 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
                 const bool ty = !tx && (nya < nxa - eps);
                 const bool both = !tx && !ty;
                 const double nxt = tx ? nxa : (ty ? nya : dmax(nxa, nya));
-                mycol[n] = unsigned(col) < unsigned(ncol) ? col : -1;
-                mylen[n] = float(nxt - ap);
-                n++;
+                put(col, float(nxt - ap));
                 ap = nxt;
                 if (tx || both) {
                   x += sx;
@@ -519,6 +520,8 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
                   nya = (vy + double(y + oy) * dy - p2y) * is;
                 }
               }
+              if (n >= kSlotCap && (sx > 0 ? x < nxb : x >= 0) && (sy > 0 ? y < nyb : y >= 0))
+                atomicExch(err, 3); // slot full before the ray left the block
             }
           }
         }
@@ -527,42 +530,41 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
         const int nr = min(kWalkLanes, nblk - r0);
         for (int jj = 0; jj < nr; jj++) {
           const int nj = __shfl_sync(0xffffffffu, n, jj);
-          const int *cc = S.col + jj * kSlotCap;
-          const float *ll = S.len + jj * kSlotCap;
+          const uint2 *cl = S.cell + jj * kSlotCap;
           int m = 0;
-          for (; m + kReplayUnroll <= nj; m += kReplayUnroll) {
-            int c4[kReplayUnroll];
-            float l4[kReplayUnroll];
-            float4 xv[kReplayUnroll][NQ];
+#if PB_FP_BATCH == 4
+          for (; m + 4 <= nj; m += 4) {
+            const uint4 p0 = *reinterpret_cast<const uint4 *>(cl + m);
+            const uint4 p1 = *reinterpret_cast<const uint4 *>(cl + m + 2);
+            const unsigned o[4] = {p0.x, p0.z, p1.x, p1.z};
+            const float l[4] = {__uint_as_float(p0.y), __uint_as_float(p0.w),
+                                __uint_as_float(p1.y), __uint_as_float(p1.w)};
+#else
+          for (; m + 2 <= nj; m += 2) {
+            const uint4 p0 = *reinterpret_cast<const uint4 *>(cl + m);
+            const unsigned o[2] = {p0.x, p0.z};
+            const float l[2] = {__uint_as_float(p0.y), __uint_as_float(p0.w)};
+#endif
+            float4 xv[PB_FP_BATCH][NQ];
 #pragma unroll
-            for (int u = 0; u < kReplayUnroll; u++) {
-              c4[u] = cc[m + u];
-              l4[u] = ll[m + u];
+            for (int u = 0; u < PB_FP_BATCH; u++)
 #pragma unroll
               for (int q = 0; q < NQ; q++)
-                xv[u][q] = (c4[u] >= 0 && vok[q])
-                               ? __ldg(reinterpret_cast<const float4 *>(vol + i64(c4[u]) * g.nz +
-                                                                        vq[q]))
-                               : make_float4(0.f, 0.f, 0.f, 0.f);
-            }
+                if (vok[q])
+                  xv[u][q] = __ldg(vb + o[u] + q * 32);
 #pragma unroll
-            for (int u = 0; u < kReplayUnroll; u++)
-              if (c4[u] >= 0) {
+            for (int u = 0; u < PB_FP_BATCH; u++)
 #pragma unroll
-                for (int q = 0; q < NQ; q++)
-                  axpy4(acc[q], xv[u][q], l4[u]);
-              }
+              for (int q = 0; q < NQ; q++)
+                if (vok[q])
+                  axpy4(acc[q], xv[u][q], l[u]);
           }
           for (; m < nj; m++) {
-            const int c1 = cc[m];
-            if (c1 < 0)
-              continue;
-            const float l1 = ll[m];
+            const uint2 p = cl[m];
 #pragma unroll
             for (int q = 0; q < NQ; q++)
               if (vok[q])
-                axpy4(acc[q],
-                      __ldg(reinterpret_cast<const float4 *>(vol + i64(c1) * g.nz + vq[q])), l1);
+                axpy4(acc[q], __ldg(vb + p.x + q * 32), __uint_as_float(p.y));
           }
         }
         __syncwarp();
@@ -936,7 +938,12 @@ __global__ void __launch_bounds__(256) pb_bp_scalar(Geom g, const float *__restr
 template <int EPI>
 int launch_fp(const Geom &g, const float *vol, float *pix, const Epi &e, int grid, int *err,
               cudaStream_t st) {
-  const bool vec4 = g.map_type == 1 && (g.nv % 4) == 0 && (g.nz % 4) == 0;
+  // float4 offsets of the columns must fit 32 bits, and a ray's block list
+  // (at most about nbx + nby entries) must fit its staging area
+  const int nblocks = (g.nx + kBlock - 1) / kBlock + (g.ny + kBlock - 1) / kBlock;
+  const bool vec4 = g.map_type == 1 && (g.nv % 4) == 0 && (g.nz % 4) == 0 &&
+                    (long long)g.nx * g.ny * (g.nz / 4) < (1ll << 32) &&
+                    nblocks + 16 <= kMaxBlocks;
   if (vec4) {
     const size_t smem = sizeof(LaneSmem) * kLaneWarps;
     for (int v0 = 0; v0 < g.nv; v0 += 256) {

@@ -116,5 +116,5 @@ def test_adam_steps_reduce_loss(cuda):
         loss = (r * r).sum()
         loss.backward()
         opt.step()
-        losses.append(float(loss))
+        losses.append(float(loss.detach()))
     assert min(losses[-5:]) < 0.3 * losses[0], losses
