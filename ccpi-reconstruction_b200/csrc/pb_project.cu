@@ -784,12 +784,14 @@ __device__ void pb_bp_stage(const Geom &g, int tx0, int ty0, int tw, int th, int
   }
 }
 
-// Vector over z (row v == slice z): each thread owns NP (column, group of
-// VW consecutive slices) pairs, VW = 8 (two float4) or 4; groups are the
-// fastest index so the lanes of a warp share a column and read its
-// staged rays as broadcasts.
+// Vector over z (row v == slice z): each thread owns NP (column, group)
+// pairs of VW = 8 (two float4) or 4 slices; groups are the fastest index so
+// the lanes of a warp share a column and read its staged rays as
+// broadcasts.  Group k holds float4 k, k + nzg, ... of the column (nzg =
+// nz / VW groups), so each load instruction of a warp covers one contiguous
+// 512-byte run of the sinogram row.
 template <int NP, int VW, int EPI>
-__global__ void __launch_bounds__(256) pb_bp_vec(Geom g, const float *__restrict__ pix,
+__global__ void __launch_bounds__(256, NP <= 2 ? 4 : (NP <= 4 ? 2 : 1)) pb_bp_vec(Geom g, const float *__restrict__ pix,
                                                  float *__restrict__ vol, Epi e, int tw, int th,
                                                  int *err) {
   extern __shared__ BpEntry ent[];
@@ -798,6 +800,7 @@ __global__ void __launch_bounds__(256) pb_bp_vec(Geom g, const float *__restrict
   const int tx0 = (blockIdx.x % ntx) * tw, ty0 = (blockIdx.x / ntx) * th;
   const int nzg = g.nz / VW;
   const int npairs = tw * th * nzg;
+  const int fstride = 4 * nzg; // floats between a group's float4s
   float4 acc[NP][NF];
   int pcol[NP], pz[NP];
 #pragma unroll
@@ -807,7 +810,7 @@ __global__ void __launch_bounds__(256) pb_bp_vec(Geom g, const float *__restrict
       acc[k][f] = make_float4(0.f, 0.f, 0.f, 0.f);
     const int p = threadIdx.x + k * blockDim.x;
     pcol[k] = (p < npairs) ? p / nzg : -1;
-    pz[k] = (p < npairs) ? (p - (p / nzg) * nzg) * VW : 0;
+    pz[k] = (p < npairs) ? (p - (p / nzg) * nzg) * 4 : 0;
   }
   for (int a0 = 0; a0 < g.na; a0 += kBpAngles) {
     __syncthreads();
@@ -829,7 +832,7 @@ __global__ void __launch_bounds__(256) pb_bp_vec(Geom g, const float *__restrict
           float4 x[NF];
 #pragma unroll
           for (int f = 0; f < NF; f++)
-            x[f] = __ldg(p + f);
+            x[f] = __ldg(p + f * nzg);
 #pragma unroll
           for (int f = 0; f < NF; f++)
             axpy4(acc[k][f], x[f], w);
@@ -849,11 +852,12 @@ __global__ void __launch_bounds__(256) pb_bp_vec(Geom g, const float *__restrict
 #pragma unroll
     for (int f = 0; f < NF; f++) {
       float4 o;
-      o.x = bp_epilogue<EPI>(acc[k][f].x, base + 4 * f + 0, e, ssq);
-      o.y = bp_epilogue<EPI>(acc[k][f].y, base + 4 * f + 1, e, ssq);
-      o.z = bp_epilogue<EPI>(acc[k][f].z, base + 4 * f + 2, e, ssq);
-      o.w = bp_epilogue<EPI>(acc[k][f].w, base + 4 * f + 3, e, ssq);
-      *reinterpret_cast<float4 *>(vol + base + 4 * f) = o;
+      const i64 at = base + i64(f) * fstride;
+      o.x = bp_epilogue<EPI>(acc[k][f].x, at + 0, e, ssq);
+      o.y = bp_epilogue<EPI>(acc[k][f].y, at + 1, e, ssq);
+      o.z = bp_epilogue<EPI>(acc[k][f].z, at + 2, e, ssq);
+      o.w = bp_epilogue<EPI>(acc[k][f].w, at + 3, e, ssq);
+      *reinterpret_cast<float4 *>(vol + at) = o;
     }
   }
   if (EPI == EPI_NORM)
