@@ -369,6 +369,9 @@ __device__ __forceinline__ int pb_column_blocks(const Geom &g, int h, double c, 
 #ifndef PB_FP_MINB
 #define PB_FP_MINB 5
 #endif
+#ifndef PB_FP_ORDER
+#define PB_FP_ORDER 0
+#endif
 #ifndef PB_FP_BATCH
 #define PB_FP_BATCH 4 // staged cells whose loads are issued together (4 or 2)
 #endif
@@ -397,8 +400,17 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
   const int nat = (g.na + kLaneWarps - 1) / kLaneWarps;
   const int ntiles = nat * g.nh;
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+#if PB_FP_ORDER == 1
+    // angle groups slow, detector columns fast: the resident CTAs trace
+    // near-parallel rays that advance through the same block columns
+    // together, so the volume strip they read stays in L2
+    const int ag = t / g.nh;
+    const int h = t - ag * g.nh;
+    const int a = ag * kLaneWarps + wib;
+#else
     const int h = t / nat;
     const int a = (t - h * nat) * kLaneWarps + wib;
+#endif
     if (a >= g.na)
       continue;
     const int ray = a * g.nh + h;
