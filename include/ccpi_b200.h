@@ -221,6 +221,25 @@ int ccpi_session_run(ccpi_session *session, int niterations);
 int ccpi_session_finish(ccpi_session *session, double *h_norms);
 void ccpi_session_destroy(ccpi_session *session);
 
+/* ccpi_solve for callers that must not allocate device memory during a
+ * solve: a host that owns all device memory through its own pool, or a
+ * loop running other streams that cannot take the device-wide
+ * synchronisation of a cudaMalloc/cudaFree pair per call.  No counterpart
+ * in the reference (its solvers allocate on the host heap per call).
+ * The solver workspace is a 16 MiB scratch area compiled into the library
+ * (per device); problems needing more (ccpi_solve_workspace_bytes) are
+ * rejected with an error naming both sizes.  The scratch needs no zeroing:
+ * every buffer is initialised by the solve.  The first call on a device
+ * looks up the scratch address (this may load the library's module): make
+ * it before any stream capture begins.  Iterations are host-driven (the
+ * CCPI_SOLVE_PLAIN schedule).  All calls on one device share the scratch,
+ * so calls that overlap in time (several host threads) race; each call
+ * blocks until done, so sequential calls are safe.  Arguments and results
+ * are as for ccpi_solve. */
+int ccpi_solve_noalloc(const ccpi_plan *plan, int alg, const float *d_sino,
+                       float *d_x, int niterations, double regularize,
+                       double *h_norms, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
