@@ -45,6 +45,9 @@ def _load():
     lib.ccpi_pb_grid.argtypes = [_c_int, _c_int, _c_int, _c_dbl, _c_int, _i32p]
     lib.ccpi_pb_reconstruct.argtypes = [_c_int, _f32p, _c_int, _c_int, _c_int, _f32p, _c_dbl,
                                         _c_int, _c_int, _c_int, _c_int, _c_dbl, _vp, _vp, _f32p]
+    lib.ccpi_pb_geometry.argtypes = [_c_int, _c_int, _c_int, _f32p, _c_dbl, _c_int, _f64p,
+                                     _f64p, _f64p, P(Geometry)]
+    lib.ccpi_pb_pack.argtypes = [_vp, _c_int, _c_int, _c_int, _c_int, _c_int, _vp, _vp]
     lib.ccpi_pb_reconstruct_batched.argtypes = [_c_int, _c_int, P(_vp), _i32p, _i32p, _i32p,
                                                 P(_vp), _f64p, _c_int, _c_int, _c_int, _vp,
                                                 P(_vp)]

@@ -187,3 +187,39 @@ def cone_plan(n_vox, vox_size, n_angles, n_det, pix_size, s2o, o2d, n_det_v=None
     origin = (-nx * vox_size / 2.0, -ny * vox_size / 2.0, -nz * vox_size / 2.0)
     return Plan("cone", ang, h, v, origin, (vox_size,) * 3, (nx, ny, nz),
                 source=(-s2o, 0.0, 0.0), detector_x=o2d)
+
+
+def parallel_api_plan(n_angles, n_v, n_h, angles_deg, rotation_centre, resolution):
+    """Plan on the grid parallelbeam.alg derives from a sinogram shape
+    (``ccpi_pb_geometry``).  Returns (plan, n_v_padded, v_offset)."""
+    ang_deg = np.ascontiguousarray(angles_deg, np.float32)
+    if ang_deg.shape != (int(n_angles),):
+        raise ValueError("angles must have n_angles entries")
+    dims = np.zeros(5, np.int32)
+    N.check(N.lib.ccpi_pb_grid(int(n_angles), int(n_v), int(n_h), float(rotation_centre),
+                               int(resolution), dims), "ccpi_pb_grid")
+    nvp, voff = int(dims[3]), int(dims[4])
+    ang = np.zeros(int(n_angles), np.float64)
+    h = np.zeros(int(n_h), np.float64)
+    v = np.zeros(nvp, np.float64)
+    g = N.Geometry()
+    N.check(N.lib.ccpi_pb_geometry(int(n_angles), int(n_v), int(n_h), ang_deg,
+                                   float(rotation_centre), int(resolution), ang, h, v,
+                                   ctypes.byref(g)), "ccpi_pb_geometry")
+    plan = Plan("parallel", ang, h, v, tuple(g.origin), tuple(g.voxel_size), (g.nx, g.ny, g.nz))
+    return plan, nvp, voff
+
+
+def pack_parallel(pixels, n_v_padded, v_offset, out=None):
+    """(n_angles, n_v, n_h) CUDA tensor -> (n_angles, n_h, n_v_padded), the
+    layout the device solvers take (``ccpi_pb_pack``)."""
+    if not (pixels.is_cuda and pixels.dtype == torch.float32 and pixels.is_contiguous()):
+        raise ValueError("pixels must be a contiguous float32 CUDA tensor")
+    na, nv, nh = pixels.shape
+    if out is None:
+        out = torch.empty((na, nh, int(n_v_padded)), device=pixels.device, dtype=torch.float32)
+    N.check(N.lib.ccpi_pb_pack(ctypes.c_void_p(pixels.data_ptr()), na, nv, nh, int(n_v_padded),
+                               int(v_offset), ctypes.c_void_p(out.data_ptr()),
+                               ctypes.c_void_p(torch.cuda.current_stream(pixels.device).cuda_stream)),
+            "ccpi_pb_pack")
+    return out

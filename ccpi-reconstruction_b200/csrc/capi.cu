@@ -385,6 +385,40 @@ int ccpi_pb_grid(int na, int nv, int nh, double cor, int ppv, int dims[5]) {
   return 0;
 }
 
+int ccpi_pb_geometry(int na, int nv, int nh, const float *angles_deg, double cor, int ppv,
+                     double *angles_rad, double *h_pixels, double *v_pixels,
+                     ccpi_geometry *geometry) {
+  ccpi::g_last_error.clear();
+  if (!angles_deg || !angles_rad || !h_pixels || !v_pixels || !geometry) {
+    set_error("ccpi_pb_geometry: null argument");
+    return 1;
+  }
+  HostGeometry G;
+  if (!pb_geometry(na, nv, nh, cor, ppv, angles_deg, G))
+    return 1;
+  std::copy(G.angles.begin(), G.angles.end(), angles_rad);
+  std::copy(G.h.begin(), G.h.end(), h_pixels);
+  std::copy(G.v.begin(), G.v.end(), v_pixels);
+  *geometry = G.g;
+  geometry->angles = angles_rad;
+  geometry->h_pixels = h_pixels;
+  geometry->v_pixels = v_pixels;
+  return 0;
+}
+
+int ccpi_pb_pack(const float *d_pixels, int na, int nv, int nh, int nv_pad, int v_offset,
+                 float *d_sino, void *stream) {
+  ccpi::g_last_error.clear();
+  if (!d_pixels || !d_sino || na < 1 || nv < 1 || nh < 1 || v_offset < 0 ||
+      v_offset + nv > nv_pad) {
+    set_error("ccpi_pb_pack: bad arguments");
+    return 1;
+  }
+  // writes every element of d_sino, padding rows included (zeros)
+  ccpi::k_pack_parallel(d_pixels, d_sino, na, nv, nh, nv_pad, v_offset, cudaStream_t(stream));
+  return ccpi::cuda_ok(cudaGetLastError(), "ccpi_pb_pack: launch") ? 0 : 2;
+}
+
 int ccpi_pb_reconstruct(int alg, const float *pixels, int na, int nv, int nh,
                         const float *angles_deg, double cor, int ppv, int niter, int nthreads,
                         int is_log, double lambda, const float *x0, double *norms,

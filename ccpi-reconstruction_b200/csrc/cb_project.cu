@@ -168,16 +168,25 @@ __device__ __forceinline__ float cb_fp_epi(float acc, i64 idx, const Epi &e, dou
 }
 
 constexpr int kFpWarps = 4;
-constexpr int kRowsPerLane = 8;
 
-template <int EPI>
+// Floats of the slice-plane table copy at the start of the forward
+// projector's shared memory (nz + 1 entries, rounded up to 4).
+__host__ __device__ inline int cb_vz_floats(int nz) { return (nz + 1 + 3) & ~3; }
+
+// RPL = detector rows per lane per pass (a pass covers 32 * RPL rows);
+// FULL: nv is a multiple of 32 * RPL (no idle rows).
+template <int EPI, int RPL, bool FULL>
 __global__ void __launch_bounds__(kFpWarps * 32)
     cb_fp_kernel(Geom g, const float *__restrict__ vol, float *__restrict__ pix, Epi e,
                  const int2 *__restrict__ hrange, int cap) {
   extern __shared__ unsigned char smem_raw[];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float *alphas = reinterpret_cast<float *>(smem_raw) + size_t(wib) * 2 * cap;
+  float *svz = reinterpret_cast<float *>(smem_raw);
+  float *alphas = svz + cb_vz_floats(g.nz) + size_t(wib) * 2 * cap;
   int *cells = reinterpret_cast<int *>(alphas + cap);
+  for (int i = threadIdx.x; i <= g.nz; i += blockDim.x)
+    svz[i] = g.vz[i];
+  __syncthreads();
   const int nrays = g.na * g.nh;
   const int nzm1 = g.nz - 1, mid = g.mid;
   const float pzbz = g.pzbz, pzbz1 = g.pzbz1, inv_dz = g.inv_dz;
@@ -248,61 +257,90 @@ __global__ void __launch_bounds__(kFpWarps * 32)
         }
       }
     }
-    // Rows, kRowsPerLane per lane per pass.
-    for (int vb = 0; vb < g.nv; vb += 32 * kRowsPerLane) {
-      float acc[kRowsPerLane], dzv[kRowsPerLane], izv[kRowsPerLane];
+    // Rows, RPL per lane per pass.  Cells [1, mfast) have every row inside
+    // the slab (c2D.cpp:99-145); the rest take the edge rules (:146-190).
+    const int mfast = min(ncom, n);
+    for (int vb = 0; vb < g.nv; vb += 32 * RPL) {
+      float acc[RPL], dzv[RPL], izv[RPL];
+      bool vok[RPL], below[RPL];
 #pragma unroll
-      for (int q = 0; q < kRowsPerLane; q++) {
+      for (int q = 0; q < RPL; q++) {
         const int v = vb + q * 32 + lane;
         acc[q] = 0.0f;
-        dzv[q] = v < g.nv ? g.dz[v] : 0.0f;
-        izv[q] = v < g.nv ? g.iz[v] : 0.0f;
+        vok[q] = v < g.nv;
+        below[q] = v < mid;
+        dzv[q] = vok[q] ? g.dz[v] : 0.0f;
+        izv[q] = vok[q] ? g.iz[v] : 0.0f;
       }
-      for (int m = 1; m < n; m++) {
+      // In [1, mfast) the regime search has shown that the lowest row's
+      // slice index is >= 1 and the highest row's < nz - 1 (c2D.cpp:45-99),
+      // so every row's k and its neighbour k -/+ 1 are inside the column.
+      int dk[RPL];
+      const float *vzq[RPL];
+#pragma unroll
+      for (int q = 0; q < RPL; q++) {
+        dk[q] = below[q] ? -1 : 1;
+        vzq[q] = svz + (below[q] ? 0 : 1);
+      }
+      for (int m = 1; m < mfast; m++) {
         const float a0 = alphas[m - 1], a1 = alphas[m];
         const int cell = cells[m - 1];
         if (cell < 0)
           continue;
         const float *col = vol + i64(cell) * g.nz;
         const float av = __fmul_rn(a0, inv_dz);
-        const bool all_rows = m < ncom;
 #pragma unroll
-        for (int q = 0; q < kRowsPerLane; q++) {
-          const int v = vb + q * 32 + lane;
-          if (v >= g.nv)
+        for (int q = 0; q < RPL; q++) {
+          if (!FULL && !vok[q])
             continue;
-          const bool inside = all_rows || (v >= min_v_all && v <= max_v_all);
-          if (inside) {
+          const int k = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[q])));
+          const float *ck = col + k;
+          const float mz = fmin_ref(__fmul_rn(vzq[q][k], izv[q]), a1);
+          acc[q] = __fadd_rn(acc[q], __fadd_rn(__fmul_rn(__ldg(ck), __fsub_rn(mz, a0)),
+                                               __fmul_rn(__ldg(ck + dk[q]), __fsub_rn(a1, mz))));
+        }
+      }
+      for (int m = max(mfast, 1); m < n; m++) {
+        const float a0 = alphas[m - 1], a1 = alphas[m];
+        const int cell = cells[m - 1];
+        if (cell < 0)
+          continue;
+        const float *col = vol + i64(cell) * g.nz;
+        const float av = __fmul_rn(a0, inv_dz);
+#pragma unroll
+        for (int q = 0; q < RPL; q++) {
+          const int v = vb + q * 32 + lane;
+          if (!vok[q])
+            continue;
+          if (v >= min_v_all && v <= max_v_all) {
             const int k = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[q])));
-            const bool below = v < mid;
-            const int kn = below ? k - 1 : k + 1;
-            if (k < 0 || k > nzm1 || kn < 0 || kn > nzm1)
+            const int kn = below[q] ? k - 1 : k + 1;
+            if (unsigned(k) > unsigned(nzm1) || unsigned(kn) > unsigned(nzm1))
               continue;
-            const float az = __fmul_rn(g.vz[below ? k : k + 1], izv[q]);
-            const float mz = fmin_ref(az, a1);
+            const float mz = fmin_ref(__fmul_rn(svz[below[q] ? k : k + 1], izv[q]), a1);
             acc[q] = __fadd_rn(acc[q], __fadd_rn(__fmul_rn(__ldg(col + k), __fsub_rn(mz, a0)),
                                                  __fmul_rn(__ldg(col + kn), __fsub_rn(a1, mz))));
           } else if (ncom >= 1) {
             if (v < min_v_all) {
               const int k = int(__fadd_rn(pzbz1, __fmul_rn(av, dzv[q]))) - 1;
               if (k > 0 && k <= nzm1) {
-                const float mz = fmin_ref(__fmul_rn(g.vz[k], izv[q]), a1);
+                const float mz = fmin_ref(__fmul_rn(svz[k], izv[q]), a1);
                 acc[q] = __fadd_rn(acc[q],
                                    __fadd_rn(__fmul_rn(__ldg(col + k), __fsub_rn(mz, a0)),
                                              __fmul_rn(__ldg(col + k - 1), __fsub_rn(a1, mz))));
               } else if (k == 0) {
-                const float mz = fmin_ref(__fmul_rn(g.vz[0], izv[q]), a1);
+                const float mz = fmin_ref(__fmul_rn(svz[0], izv[q]), a1);
                 acc[q] = __fadd_rn(acc[q], __fmul_rn(__ldg(col), __fsub_rn(mz, a0)));
               }
             } else {
               const int k = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[q])));
               if (k < nzm1 && k >= 0) {
-                const float mz = fmin_ref(__fmul_rn(g.vz[k + 1], izv[q]), a1);
+                const float mz = fmin_ref(__fmul_rn(svz[k + 1], izv[q]), a1);
                 acc[q] = __fadd_rn(acc[q],
                                    __fadd_rn(__fmul_rn(__ldg(col + k), __fsub_rn(mz, a0)),
                                              __fmul_rn(__ldg(col + k + 1), __fsub_rn(a1, mz))));
               } else if (k == nzm1) {
-                const float mz = fmin_ref(__fmul_rn(g.vz[g.nz], izv[q]), a1);
+                const float mz = fmin_ref(__fmul_rn(svz[g.nz], izv[q]), a1);
                 acc[q] = __fadd_rn(acc[q], __fmul_rn(__ldg(col + nzm1), __fsub_rn(mz, a0)));
               }
             }
@@ -311,7 +349,7 @@ __global__ void __launch_bounds__(kFpWarps * 32)
       }
       const i64 rbase = i64(ray) * g.nv;
 #pragma unroll
-      for (int q = 0; q < kRowsPerLane; q++) {
+      for (int q = 0; q < RPL; q++) {
         const int v = vb + q * 32 + lane;
         if (v < g.nv) {
           const float val = __fmul_rn(acc[q], g.dconv[i64(h) * g.nv + v]);
@@ -516,8 +554,47 @@ __global__ void __launch_bounds__(kBpThreads)
 } // namespace
 
 size_t cb_fp_smem(const Geom &g) {
-  return size_t(kFpWarps) * 2 * size_t(g.nx + g.ny + 2) * sizeof(float);
+  return (size_t(cb_vz_floats(g.nz)) + size_t(kFpWarps) * 2 * size_t(g.nx + g.ny + 2)) *
+         sizeof(float);
 }
+
+namespace {
+// Rows per lane for nv rows: fewest idle lanes, then fewest passes.
+int cb_fp_rpl(int nv) {
+#ifdef CB_FP_FORCE_RPL
+  return CB_FP_FORCE_RPL;
+#endif
+  int best = 4;
+  long long best_waste = -1;
+  for (int r : {4, 8, 12}) {
+    const long long per = 32ll * r;
+    const long long waste = ((nv + per - 1) / per) * per - nv;
+    if (best_waste < 0 || waste < best_waste || (waste == best_waste && r > best)) {
+      best = r;
+      best_waste = waste;
+    }
+  }
+  return best;
+}
+
+template <int EPI>
+void launch_cb_fp(const Geom &g, const float *vol, float *pix, const Epi &e, const int2 *hrange,
+                  int grid, cudaStream_t st) {
+  const size_t smem = cb_fp_smem(g);
+  const int cap = g.nx + g.ny + 2;
+  const int r = cb_fp_rpl(g.nv);
+  const bool full = g.nv % (32 * r) == 0;
+#define CB_FP_GO(R, F)                                                                     \
+  cb_fp_kernel<EPI, R, F><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap)
+  if (r == 12)
+    full ? CB_FP_GO(12, true) : CB_FP_GO(12, false);
+  else if (r == 8)
+    full ? CB_FP_GO(8, true) : CB_FP_GO(8, false);
+  else
+    full ? CB_FP_GO(4, true) : CB_FP_GO(4, false);
+#undef CB_FP_GO
+}
+} // namespace
 
 size_t cb_bp_smem(const Geom &g) {
   return size_t(g.nz) * sizeof(float) +
@@ -527,8 +604,12 @@ size_t cb_bp_smem(const Geom &g) {
 int cb_prepare(const Geom &g) {
   const int fp = int(cb_fp_smem(g)), bp = int(cb_bp_smem(g));
   cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
-  const void *fps[] = {(const void *)cb_fp_kernel<EPI_STORE>, (const void *)cb_fp_kernel<EPI_NORM>,
-                       (const void *)cb_fp_kernel<EPI_SIRT>, (const void *)cb_fp_kernel<EPI_MLEM>};
+#define CB_FP_ALL(R, F)                                                                    \
+  (const void *)cb_fp_kernel<EPI_STORE, R, F>, (const void *)cb_fp_kernel<EPI_NORM, R, F>,  \
+      (const void *)cb_fp_kernel<EPI_SIRT, R, F>, (const void *)cb_fp_kernel<EPI_MLEM, R, F>
+  const void *fps[] = {CB_FP_ALL(4, false), CB_FP_ALL(8, false), CB_FP_ALL(12, false),
+                       CB_FP_ALL(4, true),  CB_FP_ALL(8, true),  CB_FP_ALL(12, true)};
+#undef CB_FP_ALL
   const void *bps[] = {(const void *)cb_bp_kernel<EPI_STORE>, (const void *)cb_bp_kernel<EPI_NORM>,
                        (const void *)cb_bp_kernel<EPI_SIRT>, (const void *)cb_bp_kernel<EPI_MLEM>};
   for (const void *f : fps)
@@ -542,20 +623,18 @@ int cb_prepare(const Geom &g) {
 
 int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
                const int2 *hrange, int grid, cudaStream_t st) {
-  const size_t smem = cb_fp_smem(g);
-  const int cap = g.nx + g.ny + 2;
   switch (mode) {
   case EPI_STORE:
-    cb_fp_kernel<EPI_STORE><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap);
+    launch_cb_fp<EPI_STORE>(g, vol, pix, e, hrange, grid, st);
     break;
   case EPI_NORM:
-    cb_fp_kernel<EPI_NORM><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap);
+    launch_cb_fp<EPI_NORM>(g, vol, pix, e, hrange, grid, st);
     break;
   case EPI_SIRT:
-    cb_fp_kernel<EPI_SIRT><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap);
+    launch_cb_fp<EPI_SIRT>(g, vol, pix, e, hrange, grid, st);
     break;
   case EPI_MLEM:
-    cb_fp_kernel<EPI_MLEM><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap);
+    launch_cb_fp<EPI_MLEM>(g, vol, pix, e, hrange, grid, st);
     break;
   default:
     return 1;
