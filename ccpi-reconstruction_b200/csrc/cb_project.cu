@@ -15,11 +15,12 @@
 // Backward (cone_beam::b2D, c2D.cpp:948-1119): voxel-column gather, the
 // reference's design.  One CTA owns one xy column; it finds, angle chunk by
 // angle chunk, every (angle, detector column) ray that crosses the column
-// with the reference's entry/exit alphas (c2D.cpp:788-946), then its warps
-// spread each ray's detector rows over the column's z slices (c2D.cpp:
-// 640-751) into a shared-memory accumulator.  Shared-memory float atomics
-// make the summation order unspecified, so this projector agrees with the
-// reference to float rounding rather than bit for bit.
+// with the reference's entry/exit alphas (c2D.cpp:788-946).  cb_bp_gather
+// then has each thread form its own voxels' sums over the rays' detector
+// rows (c2D.cpp:640-751) in the reference's order, bit for bit; columns
+// taller than 1024 voxels use cb_bp_kernel, whose warps spread rows into a
+// shared-memory accumulator with float atomics (unspecified order, equal to
+// the reference to float rounding).
 #include "common.cuh"
 #include "kernels.h"
 
@@ -551,6 +552,342 @@ __global__ void __launch_bounds__(kBpThreads)
   }
 }
 
+// ---- backward, deterministic gather in the reference's summation order
+//
+// cone_beam::calc_ah_z (c2D.cpp:640-751) adds, for every voxel of a column,
+// first the band rows of every ray (list order: angle, then detector
+// column; rows ascending, each row feeding its slice k and the neighbour
+// k -/+ 1), then the edge rows of every ray (below the band descending,
+// above it ascending).  Here one CTA owns one column and each thread owns
+// NZT of its voxels.  Rays are staged per angle chunk; for a stage of
+// kGaStage rays the threads first compute, per detector row, the slice
+// index and the d_conv-scaled pixel value and record for every slice K the
+// first band row whose index reaches K (k is monotone in the row).  Each
+// voxel thread then walks exactly the rows that touch its voxel, in the
+// reference's order, so every voxel's sum is formed in the same order with
+// the same unfused float operations as the reference.
+constexpr int kGaThreads = 256;
+constexpr int kGaChunk = 64;
+constexpr int kGaRays = kBpMaxRaysPerAngle; // slots per angle
+#ifndef CB_GA_STAGE
+#define CB_GA_STAGE 4
+#endif
+constexpr int kGaStage = CB_GA_STAGE;
+
+__host__ __device__ inline int round4(int n) { return (n + 3) & ~3; }
+
+// Asynchronous global -> shared copies (cp.async), so that every row of a
+// stage is in flight at once instead of one round trip per ray.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Shared-memory layout of cb_bp_gather (offsets in 4-byte words).
+struct GaLayout {
+  int vz, dz, iz, seg_h, seg_a0, seg_a1, cnt, off, map, fr, prow, drow, total;
+  __host__ __device__ GaLayout(int nz, int nv) {
+    vz = 0;
+    dz = vz + cb_vz_floats(nz);
+    iz = dz + round4(nv);
+    seg_h = iz + round4(nv);
+    seg_a0 = seg_h + kGaChunk * kGaRays;
+    seg_a1 = seg_a0 + kGaChunk * kGaRays;
+    cnt = seg_a1 + kGaChunk * kGaRays;
+    off = cnt + round4(kGaChunk + 1);
+    map = off + round4(kGaChunk + 1);
+    fr = map + kGaChunk * kGaRays;
+    prow = fr + kGaStage * round4(nz + 2);
+    drow = prow + kGaStage * round4(nv);
+    total = drow + kGaStage * round4(nv);
+  }
+};
+
+// Stage the rays of angles [ac, ac + nac) in list order: slots per angle,
+// then a prefix over angles and a flat map.  Returns the ray count.
+__device__ int cb_ga_stage_rays(const Geom &g, int ac, int nac, double x0, double xn, double y0,
+                                double yn, int *seg_h, float *seg_a0, float *seg_a1, int *cnt,
+                                int *off, int *map, int *ovf) {
+  const int tid = threadIdx.x;
+  if (tid < nac) {
+    int c = 0;
+    cb_column_rays(g, ac + tid, x0, xn, y0, yn, [&](int h, float a0, float a1) {
+      if (c < kGaRays) {
+        const int idx = tid * kGaRays + c;
+        seg_h[idx] = h;
+        seg_a0[idx] = a0;
+        seg_a1[idx] = a1;
+      }
+      c++;
+    });
+    if (c > kGaRays) {
+      *ovf = 1;
+      c = kGaRays;
+    }
+    cnt[tid] = c;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int acc = 0;
+    for (int t = 0; t < nac; t++) {
+      off[t] = acc;
+      acc += cnt[t];
+    }
+    off[nac] = acc;
+  }
+  __syncthreads();
+  if (tid < nac)
+    for (int c = 0; c < cnt[tid]; c++)
+      map[off[tid] + c] = tid * kGaRays + c;
+  __syncthreads();
+  return off[nac];
+}
+
+template <int EPI, int NZT>
+__global__ void __launch_bounds__(kGaThreads)
+    cb_bp_gather(Geom g, const float *__restrict__ pix, float *__restrict__ vol, Epi e,
+                 int *err) {
+  extern __shared__ unsigned char smem_raw[];
+  int *W = reinterpret_cast<int *>(smem_raw);
+  const int nz = g.nz, nv = g.nv, nzm1 = nz - 1, mid = g.mid;
+  const GaLayout L(nz, nv);
+  float *svz = reinterpret_cast<float *>(W + L.vz);
+  float *sdz = reinterpret_cast<float *>(W + L.dz);
+  float *siz = reinterpret_cast<float *>(W + L.iz);
+  int *seg_h = W + L.seg_h;
+  float *seg_a0 = reinterpret_cast<float *>(W + L.seg_a0);
+  float *seg_a1 = reinterpret_cast<float *>(W + L.seg_a1);
+  int *cnt = W + L.cnt, *off = W + L.off, *map = W + L.map, *fr = W + L.fr;
+  float *prow = reinterpret_cast<float *>(W + L.prow); // staged pixel rows
+  float *drow = reinterpret_cast<float *>(W + L.drow); // their d_conv rows
+  const int frs = round4(nz + 2), prs = round4(nv);
+  __shared__ int s_minv, s_maxv, s_ovf;
+  // slice index of the first and last band row of each staged ray; the
+  // first-row table fr[K] is only written for kfirst < K <= klast
+  __shared__ int kfirst[kGaStage], klast[kGaStage];
+  const int tid = threadIdx.x;
+  const int col = blockIdx.x;
+  const int i = col / g.ny, j = col - (col / g.ny) * g.ny;
+  const double x0 = g.origin[0] + double(i) * g.size[0];
+  const double xn = g.origin[0] + double(i + 1) * g.size[0];
+  const double y0 = g.origin[1] + double(j) * g.size[1];
+  const double yn = g.origin[1] + double(j + 1) * g.size[1];
+  for (int t = tid; t <= nz; t += blockDim.x)
+    svz[t] = g.vz[t];
+  for (int t = tid; t < nv; t += blockDim.x) {
+    sdz[t] = g.dz[t];
+    siz[t] = g.iz[t];
+  }
+  if (tid == 0) {
+    s_minv = 0;
+    s_maxv = nv;
+    s_ovf = 0;
+  }
+  __syncthreads();
+  // band limits over every ray of the column (c2D.cpp:657-676)
+  for (int a = tid; a < g.na; a += blockDim.x) {
+    int lo = 0, hi = nv;
+    cb_column_rays(g, a, x0, xn, y0, yn, [&](int, float a0, float) {
+      lo = max(lo, int(ceilf(__fadd_rn(g.pzdeps, __fdiv_rn(g.z1, a0)))));
+      hi = min(hi, int(floorf(__fadd_rn(g.pzdv, __fdiv_rn(g.znm, a0)))));
+    });
+    atomicMax(&s_minv, lo);
+    atomicMin(&s_maxv, hi);
+  }
+  __syncthreads();
+  const int min_v = s_minv, max_v = s_maxv;
+  const int nb = max_v - min_v;
+  // 16-byte copies need 16-byte aligned rows (nv a multiple of 4)
+  const bool vec16 = (nv & 3) == 0;
+  const int lo_end = min(mid, max_v);         // lower band rows [min_v, lo_end)
+  const int up_begin = max(mid, min_v);       // upper band rows [up_begin, max_v)
+  const float pzbz = g.pzbz, pzbz1 = g.pzbz1, inv_dz = g.inv_dz;
+  float acc[NZT], vzk[NZT], vzk1[NZT];
+#pragma unroll
+  for (int q = 0; q < NZT; q++) {
+    const int K = min(tid + q * kGaThreads, nzm1);
+    acc[q] = 0.0f;
+    vzk[q] = svz[K];
+    vzk1[q] = svz[K + 1];
+  }
+
+  // ---- band rows of every ray (c2D.cpp:680-713)
+  for (int ac = 0; nb > 0 && ac < g.na; ac += kGaChunk) {
+    const int nac = min(kGaChunk, g.na - ac);
+    const int nseg = cb_ga_stage_rays(g, ac, nac, x0, xn, y0, yn, seg_h, seg_a0, seg_a1, cnt,
+                                      off, map, &s_ovf);
+    for (int s0 = 0; s0 < nseg; s0 += kGaStage) {
+      const int ns = min(kGaStage, nseg - s0);
+      // start the copies of the stage's pixel and d_conv rows (band only)
+      for (int s = 0; s < ns; s++) {
+        const int m = map[s0 + s];
+        const int a = ac + m / kGaRays, h = seg_h[m];
+        const float *prw = pix + (i64(a) * g.nh + h) * nv;
+        const float *drw = g.dconv + i64(h) * nv;
+        float *pr = prow + s * prs, *dr = drow + s * prs;
+        if (vec16) {
+          for (int v = (min_v & ~3) + 4 * tid; v < max_v; v += 4 * blockDim.x) {
+            cp_async16(pr + v, prw + v);
+            cp_async16(dr + v, drw + v);
+          }
+        } else {
+          for (int v = min_v + tid; v < max_v; v += blockDim.x) {
+            cp_async4(pr + v, prw + v);
+            cp_async4(dr + v, drw + v);
+          }
+        }
+      }
+      // meanwhile: first band row of every slice index, per ray
+      for (int s = 0; s < ns; s++) {
+        const float av = __fmul_rn(seg_a0[map[s0 + s]], inv_dz);
+        int *f = fr + s * frs;
+        for (int v = min_v + tid; v < max_v; v += blockDim.x) {
+          const int k = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[v])));
+          if (v == min_v)
+            kfirst[s] = k;
+          else {
+            const int kp = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[v - 1])));
+            for (int K = max(kp + 1, 0); K <= min(k, nz + 1); K++)
+              f[K] = v;
+          }
+          if (v == max_v - 1)
+            klast[s] = k;
+        }
+      }
+      cp_async_wait_all();
+      __syncthreads();
+      for (int s = 0; s < ns; s++) {
+        const int m = map[s0 + s];
+        const float a0 = seg_a0[m], a1 = seg_a1[m];
+        const int *f = fr + s * frs;
+        const float *pr = prow + s * prs, *dr = drow + s * prs;
+        const int kf = kfirst[s], kl = klast[s];
+        // first band row whose slice index reaches K
+        auto first = [&](int K) { return K <= kf ? min_v : (K > kl ? max_v : f[max(K, 0)]); };
+#pragma unroll
+        for (int q = 0; q < NZT; q++) {
+          const int K = tid + q * kGaThreads;
+          if (K >= nz)
+            continue;
+          // lower band: rows with k in {K, K+1}; k == K feeds K, k == K+1
+          // feeds its neighbour k - 1 == K
+          const int fk = first(K), fk1 = first(K + 1);
+          for (int v = fk, ve = min(first(K + 2), lo_end); v < ve; v++) {
+            const float p = __fmul_rn(pr[v], dr[v]);
+            if (v < fk1) {
+              const float mz = fmin_ref(__fmul_rn(vzk[q], siz[v]), a1);
+              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(mz, a0)));
+            } else {
+              const float mz = fmin_ref(__fmul_rn(vzk1[q], siz[v]), a1);
+              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(a1, mz)));
+            }
+          }
+          // upper band: rows with k in {K-1, K}; k == K-1 feeds k + 1 == K
+          for (int v = max(first(K - 1), up_begin), ve = min(fk1, max_v); v < ve; v++) {
+            const float p = __fmul_rn(pr[v], dr[v]);
+            if (v < fk) {
+              const float mz = fmin_ref(__fmul_rn(vzk[q], siz[v]), a1);
+              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(a1, mz)));
+            } else {
+              const float mz = fmin_ref(__fmul_rn(vzk1[q], siz[v]), a1);
+              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(mz, a0)));
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+
+  // ---- edge rows of every ray (c2D.cpp:715-750)
+  if (min_v > 0 || max_v < nv) {
+    for (int ac = 0; ac < g.na; ac += kGaChunk) {
+      const int nac = min(kGaChunk, g.na - ac);
+      const int nseg = cb_ga_stage_rays(g, ac, nac, x0, xn, y0, yn, seg_h, seg_a0, seg_a1, cnt,
+                                        off, map, &s_ovf);
+      for (int s = 0; s < nseg; s++) {
+        const int m = map[s];
+        const int a = ac + m / kGaRays, h = seg_h[m];
+        const float a0 = seg_a0[m], a1 = seg_a1[m];
+        const float av = __fmul_rn(a0, inv_dz);
+        const float *prw = pix + (i64(a) * g.nh + h) * nv;
+        const float *drw = g.dconv + i64(h) * nv;
+#pragma unroll
+        for (int q = 0; q < NZT; q++) {
+          const int K = tid + q * kGaThreads;
+          if (K >= nz)
+            continue;
+          for (int v = min(min_v, nv) - 1; v >= 0; v--) {
+            const int k = int(__fadd_rn(pzbz1, __fmul_rn(av, sdz[v]))) - 1;
+            if (k < K)
+              break; // k only falls as v falls (and k < 0 ends the reference's loop)
+            if (k > K + 1)
+              continue;
+            const float p = __fmul_rn(__ldg(prw + v), __ldg(drw + v));
+            if (k > 0) {
+              const float mz = fmin_ref(__fmul_rn(svz[k], siz[v]), a1);
+              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, k == K ? __fsub_rn(mz, a0)
+                                                             : __fsub_rn(a1, mz)));
+            } else if (K == 0) {
+              const float mz = fmin_ref(__fmul_rn(svz[0], siz[v]), a1);
+              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(mz, a0)));
+            }
+          }
+          for (int v = max(max_v, 0); v < nv; v++) {
+            const int k = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[v])));
+            if (k > K || k > nzm1)
+              break; // k only rises with v (and k > nz - 1 ends the reference's loop)
+            if (k < K - 1)
+              continue;
+            const float p = __fmul_rn(__ldg(prw + v), __ldg(drw + v));
+            const float mz = fmin_ref(__fmul_rn(svz[k + 1], siz[v]), a1);
+            if (k == K)
+              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(mz, a0)));
+            else if (k < nzm1)
+              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(a1, mz)));
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0 && s_ovf)
+    atomicExch(err, 2);
+  double ssq = 0.0;
+  const i64 base = i64(col) * nz;
+#pragma unroll
+  for (int q = 0; q < NZT; q++) {
+    const int K = tid + q * kGaThreads;
+    if (K >= nz)
+      continue;
+    const float v = acc[q];
+    float o = v;
+    if (EPI == EPI_NORM) {
+      ssq += double(v) * double(v);
+    } else if (EPI == EPI_SIRT) {
+      const float t = __fadd_rn(e.x[base + K], __fmul_rn(1.0f, __fmul_rn(v, e.w[base + K])));
+      o = (t < 0.0f) ? 0.0f : t;
+    } else if (EPI == EPI_MLEM) {
+      const float t = __fmul_rn(e.x[base + K], __fmul_rn(e.w[base + K], v));
+      o = (t < 0.0f) ? 0.0f : t;
+    }
+    vol[base + K] = o;
+  }
+  if (EPI == EPI_NORM) {
+    __shared__ double red[kGaThreads / 32];
+    const double t = cta_sum<kGaThreads / 32>(ssq, red);
+    if (threadIdx.x == 0)
+      e.partials[blockIdx.x] = t;
+  }
+}
+
 } // namespace
 
 size_t cb_fp_smem(const Geom &g) {
@@ -596,13 +933,27 @@ void launch_cb_fp(const Geom &g, const float *vol, float *pix, const Epi &e, con
 }
 } // namespace
 
-size_t cb_bp_smem(const Geom &g) {
+namespace {
+size_t cb_bp_atomic_smem(const Geom &g) {
   return size_t(g.nz) * sizeof(float) +
          size_t(kBpAngleChunk) * kBpMaxRaysPerAngle * (sizeof(int) + 2 * sizeof(float));
 }
+size_t cb_bp_gather_smem(const Geom &g) { return size_t(GaLayout(g.nz, g.nv).total) * 4; }
+// voxels per thread of the deterministic gather, 0 if it does not apply
+int cb_bp_gather_nzt(const Geom &g) {
+  if (cb_bp_gather_smem(g) > 200 * 1024)
+    return 0;
+  return g.nz <= kGaThreads ? 1 : g.nz <= 2 * kGaThreads ? 2 : g.nz <= 4 * kGaThreads ? 4 : 0;
+}
+} // namespace
+
+size_t cb_bp_smem(const Geom &g) {
+  return cb_bp_gather_nzt(g) ? cb_bp_gather_smem(g) : cb_bp_atomic_smem(g);
+}
 
 int cb_prepare(const Geom &g) {
-  const int fp = int(cb_fp_smem(g)), bp = int(cb_bp_smem(g));
+  const int fp = int(cb_fp_smem(g)), bp = int(cb_bp_atomic_smem(g));
+  const int ga = int(cb_bp_gather_smem(g));
   cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
 #define CB_FP_ALL(R, F)                                                                    \
   (const void *)cb_fp_kernel<EPI_STORE, R, F>, (const void *)cb_fp_kernel<EPI_NORM, R, F>,  \
@@ -618,6 +969,16 @@ int cb_prepare(const Geom &g) {
   for (const void *f : bps)
     if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bp) != cudaSuccess)
       e2 = cudaErrorInvalidValue;
+  if (cb_bp_gather_nzt(g)) {
+#define CB_GA_ALL(Z)                                                                       \
+  (const void *)cb_bp_gather<EPI_STORE, Z>, (const void *)cb_bp_gather<EPI_NORM, Z>,        \
+      (const void *)cb_bp_gather<EPI_SIRT, Z>, (const void *)cb_bp_gather<EPI_MLEM, Z>
+    const void *gas[] = {CB_GA_ALL(1), CB_GA_ALL(2), CB_GA_ALL(4)};
+#undef CB_GA_ALL
+    for (const void *f : gas)
+      if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ga) != cudaSuccess)
+        e2 = cudaErrorInvalidValue;
+  }
   return (e1 == cudaSuccess && e2 == cudaSuccess) ? 0 : 1;
 }
 
@@ -642,22 +1003,41 @@ int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi 
   return 0;
 }
 
+namespace {
+template <int EPI>
+void launch_cb_bp(const Geom &g, const float *pix, float *vol, const Epi &e, int *err,
+                  cudaStream_t st) {
+  const int ncol = g.nx * g.ny;
+  switch (cb_bp_gather_nzt(g)) {
+  case 1:
+    cb_bp_gather<EPI, 1><<<ncol, kGaThreads, cb_bp_gather_smem(g), st>>>(g, pix, vol, e, err);
+    break;
+  case 2:
+    cb_bp_gather<EPI, 2><<<ncol, kGaThreads, cb_bp_gather_smem(g), st>>>(g, pix, vol, e, err);
+    break;
+  case 4:
+    cb_bp_gather<EPI, 4><<<ncol, kGaThreads, cb_bp_gather_smem(g), st>>>(g, pix, vol, e, err);
+    break;
+  default:
+    cb_bp_kernel<EPI><<<ncol, kBpThreads, cb_bp_atomic_smem(g), st>>>(g, pix, vol, e, err);
+  }
+}
+} // namespace
+
 int cb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
                 int *err, cudaStream_t st) {
-  const size_t smem = cb_bp_smem(g);
-  const int ncol = g.nx * g.ny;
   switch (mode) {
   case EPI_STORE:
-    cb_bp_kernel<EPI_STORE><<<ncol, kBpThreads, smem, st>>>(g, pix, vol, e, err);
+    launch_cb_bp<EPI_STORE>(g, pix, vol, e, err, st);
     break;
   case EPI_NORM:
-    cb_bp_kernel<EPI_NORM><<<ncol, kBpThreads, smem, st>>>(g, pix, vol, e, err);
+    launch_cb_bp<EPI_NORM>(g, pix, vol, e, err, st);
     break;
   case EPI_SIRT:
-    cb_bp_kernel<EPI_SIRT><<<ncol, kBpThreads, smem, st>>>(g, pix, vol, e, err);
+    launch_cb_bp<EPI_SIRT>(g, pix, vol, e, err, st);
     break;
   case EPI_MLEM:
-    cb_bp_kernel<EPI_MLEM><<<ncol, kBpThreads, smem, st>>>(g, pix, vol, e, err);
+    launch_cb_bp<EPI_MLEM>(g, pix, vol, e, err, st);
     break;
   default:
     return 1;

@@ -77,3 +77,26 @@ def test_setup_geometry_dicts():
                  "output_volume_y": 160, "output_volume_z": 8}
     d = alg.pb_setup_geometry_from_image(np.zeros((24, 20, 7)), np.zeros(16), 1)
     assert d["n_h"] == 24 and d["n_v"] == 8 and d["output_volume_z"] == 7
+
+
+@pytest.mark.parametrize("na,nv,nh,cor,ppv", [(30, 7, 40, 0.0, 1), (45, 16, 64, 33.25, 2),
+                                              (12, 5, 33, 16.0, 1)])
+def test_pb_geometry_matches_oracle_front_end(na, nv, nh, cor, ppv):
+    """ccpi_pb_geometry gives the geometry the oracle's restatement of the
+    Diamond front-end gives (grid, detector coordinates, angles)."""
+    import ctypes
+    import oracle as O
+    from ccpi.reconstruction import _native as N
+    deg = np.linspace(0, 180, na, endpoint=False).astype(np.float32)
+    dims = np.zeros(5, np.int32)
+    assert N.lib.ccpi_pb_grid(na, nv, nh, cor, ppv, dims) == 0
+    ang = np.zeros(na)
+    h = np.zeros(nh)
+    v = np.zeros(int(dims[3]))
+    g = N.Geometry()
+    assert N.lib.ccpi_pb_geometry(na, nv, nh, deg, cor, ppv, ang, h, v, ctypes.byref(g)) == 0
+    og, nvp, voff = O.parallel_api_geometry(na, nv, nh, deg, cor, ppv)
+    assert (g.nx, g.ny, g.nz) == tuple(og.shape) and (nvp, voff) == (dims[3], dims[4])
+    assert np.array_equal(ang, og.angles) and np.array_equal(h, og.h_pixels)
+    assert np.array_equal(v, og.v_pixels)
+    assert tuple(g.origin) == tuple(og.origin) and tuple(g.voxel_size) == tuple(og.size)

@@ -9,7 +9,7 @@ source and detector 31.25 mm from the axis), batch of 8 volumes.  Checks:
     voxels against autograd's gradient (L is quadratic, so the central
     difference is exact up to FP32 rounding of the projections);
   * the backward pass against the reference's own back projector
-    (cone_beam::b2D, Core/src/c2D.cpp:1052-1119), max-relative <= 1e-5;
+    (cone_beam::b2D, Core/src/c2D.cpp:1052-1119): bit for bit;
   * a few Adam steps on the loss decrease it.
 """
 import numpy as np
@@ -96,7 +96,7 @@ def test_backward_matches_reference_backprojector(cuda):
     out = project(x, p)
     out.backward(torch.from_numpy(w).to(cuda))
     ref = O.ref_backward(g, w)
-    assert max_rel(x.grad.cpu().numpy(), ref) <= 1e-5
+    assert np.array_equal(x.grad.cpu().numpy(), ref), max_rel(x.grad.cpu().numpy(), ref)
 
 
 def test_adam_steps_reduce_loss(cuda):

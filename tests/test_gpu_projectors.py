@@ -1,10 +1,11 @@
 """CUDA projectors against the reference's golden outputs and the oracle.
 
-Parallel-beam forward and back projection and cone-beam forward projection
-are expected to equal the reference bit for bit (same walk decisions, same
-float rounding and summation order); the cone back projector accumulates
-in shared memory in unspecified order and must agree to the projector
-tolerance, max|new - ref| / max|ref| <= 1e-5.
+Parallel- and cone-beam forward and back projection are expected to equal
+the reference bit for bit (same walk decisions, same float rounding and
+summation order).  The one exception is the cone back projector for columns
+taller than 1024 voxels, which accumulates with shared-memory atomics in
+unspecified order and must agree to the projector tolerance,
+max|new - ref| / max|ref| <= 1e-5.
 """
 import numpy as np
 import pytest
@@ -51,7 +52,7 @@ def test_cone_vs_reference(name, cuda):
     fp = run(p, "forward", d["vol"], cuda)
     bp = run(p, "backward", d["pix"], cuda)
     assert np.array_equal(fp, d["fp"]), max_rel(fp, d["fp"])
-    assert max_rel(bp, d["bp"]) <= TOL
+    assert np.array_equal(bp, d["bp"]), max_rel(bp, d["bp"])
 
 
 @pytest.mark.parametrize("seed", [0, 1, 2])
@@ -97,6 +98,18 @@ def test_cone_random_geometries_vs_oracle(seed, cuda):
     # an odd detector puts a row exactly at the source height, where the
     # reference's own arithmetic yields NaN (it reports "Oops"): same NaNs
     assert np.array_equal(run(p, "forward", vol, cuda), O.forward(g, vol), equal_nan=True)
+    assert np.array_equal(run(p, "backward", pix, cuda), O.backward(g, pix), equal_nan=True)
+
+
+def test_cone_tall_columns_atomic_path(cuda):
+    """Columns of more than 1024 voxels take the shared-atomic back
+    projector: equal to the oracle within the projector tolerance."""
+    from ccpi.reconstruction.device import Plan
+    rng = np.random.default_rng(7)
+    g = O.cone_geometry((4, 4, 1100), 1.0, 12, 16, 0.8, 50.0, 50.0, n_det_v=1100)
+    p = Plan("cone", g.angles, g.h_pixels, g.v_pixels, g.origin, g.size, g.shape,
+             source=g.source, detector_x=g.detector_x)
+    pix = rng.random(g.sino_shape).astype(np.float32)
     b_gpu, b_ref = run(p, "backward", pix, cuda), O.backward(g, pix)
     ok = np.isfinite(b_ref)
     assert np.array_equal(np.isfinite(b_gpu), ok)
