@@ -54,6 +54,11 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--small", action="store_true", help="profiling-size workload")
+    ap.add_argument("--workload", default="sirt",
+                    choices=["sirt", "cone-cgls", "uneven", "autograd"],
+                    help="sirt: the default line; the others print their own line")
+    ap.add_argument("--fp64-check", action="store_true",
+                    help="cone-cgls: also solve a 1/4-scale copy against the FP64 oracle")
     args = ap.parse_args()
     if args.small:
         g = globals()
@@ -224,11 +229,398 @@ def run_reference(args):
         "e2e": {"value": v, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+# ------------------------------------------------------- other workloads
+def ellipsoids(torch, dev, n, count, axes, seed, dtype=None):
+    """Sum of `count` seeded random ellipsoids in an n^3 grid: centres in
+    the inner 60 %, semi-axes U[axes] voxels, random orientation, densities
+    U[0.1, 1] (draw order: centre, axes, rotation, density, per ellipsoid)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    c = torch.arange(n, device=dev, dtype=torch.float32) + 0.5 - n / 2
+    X = c.view(n, 1, 1)
+    Y = c.view(1, n, 1)
+    Z = c.view(1, 1, n)
+    vol = torch.zeros((n, n, n), device=dev, dtype=torch.float32)
+    for _ in range(count):
+        cen = rng.uniform(-0.3, 0.3, 3) * n
+        ax = rng.uniform(axes[0], axes[1], 3)
+        q, _r = np.linalg.qr(rng.standard_normal((3, 3)))
+        den = rng.uniform(0.1, 1.0)
+        dx, dy, dz = X - float(cen[0]), Y - float(cen[1]), Z - float(cen[2])
+        acc = None
+        for k in range(3):
+            u = (dx * float(q[0, k]) + dy * float(q[1, k]) + dz * float(q[2, k])) / float(ax[k])
+            acc = u * u if acc is None else acc + u * u
+        vol += (acc <= 1.0).float() * float(den)
+        del acc
+    return vol
+
+
+def cuda_time(torch, fn, reps=1):
+    s = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(reps):
+        fn()
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1000.0 / reps
+
+
+def line_common(args, workload, value, unit, t_step, cfg, **extra):
+    d = {"metric": METRIC, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+         "warmup": args.warmup, "ms_per_step": 1000.0 * t_step, "higher_is_better": True,
+         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+         "config": dict({"workload": workload}, **cfg)}
+    d.update(extra)
+    return d
+
+
+def run_cone_cgls(args):
+    """512^3 cone-beam CGLS: 40 seeded ellipsoids (semi-axes 10-120 voxels)
+    at 1 mm, 720 angles over [0, 2 pi), 768 x 768 detector of 0.8 mm pixels,
+    source and detector 500 mm from the axis, Poisson noise at 5e3 photons,
+    CGLS on the explicit 512^3 grid.  A step is one CGLS iteration (one
+    graph launch)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from ccpi.reconstruction import _native as N
+    from ccpi.reconstruction.device import Session, cone_plan
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n, na, nd = 512, 720, 768
+    plan = cone_plan(n, 1.0, na, nd, 0.8, 500.0, 500.0)
+    vol = ellipsoids(torch, dev, n, 40, (10.0, 120.0), seed=3)
+    clean = plan.forward(vol)
+    del vol
+    mu = 3.0 / float(clean.max())
+    gen = torch.Generator(device=dev).manual_seed(3)
+    i0 = 5.0e3
+    counts = torch.poisson(i0 * torch.exp(-mu * clean), generator=gen)
+    sino = -torch.log(torch.clamp(counts, min=1.0) / i0)
+    del counts, clean
+    V, P = n ** 3, na * nd * nd
+    x = torch.zeros(plan.shape, device=dev)
+    sess = Session(plan, N.CGLS, sino, x, args.warmup + args.steps)
+    sess.run(args.warmup)
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    t = cuda_time(torch, lambda: sess.run(args.steps))
+    clk = clocks.stop()
+    norms = sess.finish()
+    sess.close()
+    t_it = t / args.steps
+    tmp_p = torch.empty_like(sino)
+    t_fp = cuda_time(torch, lambda: plan.forward(x, tmp_p), 2)
+    t_bp = cuda_time(torch, lambda: plan.backward(sino, x), 2)
+    del tmp_p
+    # plain: host-driven iterations (the per-iteration launch sequence with
+    # the step scalars read back each iteration)
+    xp = torch.zeros(plan.shape, device=dev)
+    t_plain2 = cuda_time(torch, lambda: plan.solve(N.CGLS, sino, xp, 2, plain=True))
+    t_plain1 = cuda_time(torch, lambda: plan.solve(N.CGLS, sino, xp, 1, plain=True))
+    t_plain_it = max(t_plain2 - t_plain1, 1e-9)
+    del xp
+    # e2e: pinned host sinogram in, host volume out, through ccpi_solve
+    host_s = torch.empty(sino.shape, dtype=torch.float32, pin_memory=True)
+    host_s.copy_(sino)
+    host_x = torch.empty(plan.shape, dtype=torch.float32, pin_memory=True)
+    del sino
+    torch.cuda.empty_cache()
+
+    def e2e():
+        ds = host_s.to(dev, non_blocking=True)
+        dx = torch.zeros(plan.shape, device=dev)
+        plan.solve(N.CGLS, ds, dx, args.steps)
+        host_x.copy_(dx)
+    t0 = time.perf_counter()
+    e2e()
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    peak, peak_kind = load_peaks()
+    it_bytes = 4.0 * (7 * V + 4 * P)
+    fp64 = cone_fp64_check(torch, dev) if args.fp64_check else None
+    cpu = None if args.no_cpu else cone_cpu_sample(n, na, nd)
+    print(json.dumps(line_common(
+        args, "cone-beam CGLS, 512^3 ellipsoid phantom (40), 720 angles over 2 pi, 768x768 "
+              "detector at 0.8 mm, source/detector 500 mm, Poisson 5e3, explicit 512^3 grid",
+        1.0 / t_it, "iter/s", t_it,
+        {"grid": [n, n, n], "angles": na, "detector": [nd, nd], "mu": mu,
+         "l2": "inputs larger than L2 (sinogram 1.7 GB, volume 537 MB)",
+         "form": "one CUDA graph per iteration"},
+        fp_ms=1000 * t_fp, bp_ms=1000 * t_bp,
+        projector_rays_per_s={"forward": P / t_fp, "backward": P / t_bp},
+        plain_iter_per_s=1.0 / t_plain_it, batched_over_plain=t_plain_it / t_it,
+        roofline={"bound": "hbm", "kernel": "one CGLS iteration", "achieved": it_bytes / t_it / 1e9,
+                  "peak": peak, "unit": "GB/s", "frac": it_bytes / t_it / 1e9 / peak,
+                  "peak_kind": peak_kind, "algorithmic_bytes_per_iteration": it_bytes,
+                  "traffic": None},
+        e2e={"value": args.steps / t_e2e, "unit": "iter/s",
+             "h2d_bytes_per_step": 4.0 * P / args.steps, "d2h_bytes_per_step": 4.0 * V / args.steps,
+             "call": "ccpi_solve(CGLS, %d iterations) with pinned host sinogram and volume" % args.steps},
+        gpu_launches=None, clocks=clk, residual_norms=[float(v) for v in norms[-3:]],
+        fp64_oracle=fp64, cpu_baseline=cpu)))
+
+
+def cone_fp64_check(torch, dev):
+    """GPU CGLS against the FP64 oracle on a 1/4-scale copy of the cone
+    workload (128^3 at 4 mm, 180 angles, 192^2 detector at 3.2 mm)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from ccpi.reconstruction.device import cone_plan
+    n, na, nd, it = 128, 180, 192, 30
+    plan = cone_plan(n, 4.0, na, nd, 3.2, 500.0, 500.0)
+    vol = ellipsoids(torch, dev, n, 40, (2.5, 30.0), seed=3)
+    sino = plan.forward(vol)
+    x = torch.zeros(plan.shape, device=dev)
+    plan.solve(0, sino, x, it)
+    g = O.cone_geometry(n, 4.0, na, nd, 3.2, 500.0, 500.0)
+    r64 = O.solve(g, 0, sino.cpu().numpy().astype(np.float64), it, fp64=True)
+    xs = x.cpu().numpy().astype(np.float64)
+    return {"case": "128^3, 180 angles, 192^2 detector, 30 CGLS iterations, noiseless",
+            "rel_l2": float(np.linalg.norm(xs - r64) / np.linalg.norm(r64))}
+
+
+def cone_cpu_sample(n, na, nd):
+    """The reference's cone CGLS (oracle/_ref, explicit 512^3 grid) on 8 of
+    the 720 angles with the full detector: t(2 iterations) - t(1) scaled by
+    90 to one iteration of the full workload."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.reference_available():
+        return None
+    g = O.cone_geometry(n, 1.0, 8, nd, 0.8, 500.0, 500.0)
+    g.angles = np.arange(8) * (2 * math.pi / na) * (na // 8)
+    rng = np.random.default_rng(3)
+    sino = rng.random(g.sino_shape).astype(np.float32)
+    threads = os.cpu_count() or 1
+    times = []
+    for it in (1, 2):
+        t0 = time.perf_counter()
+        with O.quiet():
+            O.ref_cb_solve_explicit(g, 0, sino, it, nthreads=threads)
+        times.append(time.perf_counter() - t0)
+    t_iter = max(times[1] - times[0], 1e-9) * (na / 8)
+    return {"value": 1.0 / t_iter, "unit": "iter/s", "cores": threads, "kind": "reference",
+            "sample": "reference cone CGLS (Core/src cgls_3d on an explicit 512^3 grid) on 8 of "
+                      "720 angles x 768^2 detector; t(2 iter) - t(1 iter) scaled x90"}
+
+
+def uneven_problems(torch, dev, count=64):
+    """64 seeded uneven parallel-beam problems (SeedSequence(4).spawn(64)):
+    width w ~ U{64..384}, rows nz ~ U{8..64}, angles ~ U{90..900} over
+    [0, pi), round(1.5 w) detector columns, lambda log-uniform in
+    [1e-3, 1e-1]; 10 ellipses per slice projected on a w x w x nz grid,
+    Gaussian noise of 2 % of the largest value.  Returns host pixel arrays
+    (n_angles, n_v, n_h) with degrees and lambdas."""
+    import numpy as np
+    from ccpi.reconstruction.device import Plan
+    out = []
+    for ss in np.random.SeedSequence(4).spawn(count):
+        rng = np.random.default_rng(ss)
+        w = int(rng.integers(64, 385))
+        nz = int(rng.integers(8, 65))
+        na = int(rng.integers(90, 901))
+        nh = int(round(1.5 * w))
+        lam = float(np.exp(rng.uniform(np.log(1e-3), np.log(1e-1))))
+        deg = np.linspace(0.0, 180.0, na, endpoint=False).astype(np.float32)
+        c = torch.arange(w, device=dev, dtype=torch.float32) + 0.5 - w / 2
+        X, Y = c.view(w, 1), c.view(1, w)
+        vol = torch.zeros((w, w, nz), device=dev)
+        for k in range(nz):
+            sl = torch.zeros((w, w), device=dev)
+            for _ in range(10):
+                cx, cy = rng.uniform(-0.4, 0.4, 2) * w
+                a, b = rng.uniform(0.04, 0.31, 2) * w
+                th = rng.uniform(0, math.pi)
+                d = rng.uniform(0.1, 1.0)
+                xr = (X - cx) * math.cos(th) + (Y - cy) * math.sin(th)
+                yr = -(X - cx) * math.sin(th) + (Y - cy) * math.cos(th)
+                sl += ((xr / a) ** 2 + (yr / b) ** 2 <= 1.0).float() * d
+            vol[:, :, k] = sl
+        ang = math.pi * (deg.astype(np.float64) / 180.0)
+        h = np.arange(nh) - (nh - 1) / 2.0
+        v = np.arange(nz) - (nz - 1) / 2.0
+        p = Plan("parallel", ang, h, v, (-w / 2, -w / 2, -nz / 2), (1.0, 1.0, 1.0), (w, w, nz))
+        s = p.forward(vol).cpu().numpy()  # (na, nh, nz)
+        p.close()
+        s = s + rng.normal(0.0, 0.02 * np.abs(s).max(), s.shape).astype(np.float32)
+        out.append(dict(pixels=np.ascontiguousarray(s.transpose(0, 2, 1), np.float32),
+                        deg=deg, lam=lam))
+    return out
+
+
+def run_uneven(args):
+    """64 uneven CGLS-Tikhonov and CGLS-TV problems, 40 iterations, one
+    CUDA graph per iteration holding all 64 problems.  A step is one
+    iteration of the whole batch."""
+    import numpy as np
+    import torch
+
+    from ccpi.reconstruction.device import pack_parallel, parallel_api_plan, solve_batched
+    from ccpi.reconstruction.parallelbeam import alg as A
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    probs = uneven_problems(torch, dev)
+    niter = 40
+    plans, sinos = [], []
+    for p in probs:
+        na, nv, nh = p["pixels"].shape
+        plan, nvp, voff = parallel_api_plan(na, nv, nh, p["deg"], 0.0, 1)
+        plans.append(plan)
+        sinos.append(pack_parallel(torch.from_numpy(p["pixels"]).to(dev), nvp, voff))
+    lams = [p["lam"] for p in probs]
+    V = sum(int(np.prod(pl.shape)) for pl in plans)
+    P = sum(int(np.prod(pl.sino_shape)) for pl in plans)
+    res = {}
+    clocks = Clocks(0)
+    for alg, name in ((3, "cgls_tikhonov"), (4, "cgls_TVreg")):
+        xs = [torch.zeros(pl.shape, device=dev) for pl in plans]
+        solve_batched(plans, alg, sinos, xs, 2, lams)  # warm-up (graph, caches)
+        xs = [torch.zeros(pl.shape, device=dev) for pl in plans]
+        t = cuda_time(torch, lambda: solve_batched(plans, alg, sinos, xs, niter, lams))
+        # plain: problems one at a time, host-driven iterations, on a sample
+        sample = list(range(0, len(plans), 8))
+        tp = 0.0
+        for i in sample:
+            y = torch.zeros(plans[i].shape, device=dev)
+            tp += cuda_time(torch, lambda: plans[i].solve(alg, sinos[i], y, niter, lams[i],
+                                                         plain=True))
+        t_plain = tp * len(plans) / len(sample)
+        res[name] = {"batched_s": t, "plain_s": t_plain}
+    clk = clocks.stop()
+    # e2e through the host-buffer batched call (Tikhonov)
+    t0 = time.perf_counter()
+    A.reconstruct_batched("cgls_tikhonov", [p["pixels"] for p in probs], [p["deg"] for p in probs],
+                          0.0, 1, niter, 1, True, regularize=lams)
+    t_e2e = time.perf_counter() - t0
+    t_tik = res["cgls_tikhonov"]["batched_s"]
+    peak, peak_kind = load_peaks()
+    it_bytes = 4.0 * (12 * V + 4 * P)
+    cpu = None if args.no_cpu else uneven_cpu_sample(probs)
+    print(json.dumps(line_common(
+        args, "64 uneven parallel-beam CGLS-Tikhonov and CGLS-TV problems (64^2x8 .. 384^2x64 "
+              "volumes, 90-900 angles, 1.5x detector columns, 2% noise), 40 iterations, all 64 "
+              "in one graph per iteration", niter / t_tik, "iter/s", t_tik / niter,
+        {"problems": len(probs), "voxels": V, "pixels": P, "iterations": niter,
+         "form": "batched: 64 problems per graph launch (16 branch streams)"},
+        tv_iter_per_s=niter / res["cgls_TVreg"]["batched_s"],
+        plain_iter_per_s={k: niter / v["plain_s"] for k, v in res.items()},
+        batched_over_plain={k: v["plain_s"] / v["batched_s"] for k, v in res.items()},
+        roofline={"bound": "hbm", "kernel": "one regularised CGLS iteration of the batch",
+                  "achieved": it_bytes / (t_tik / niter) / 1e9, "peak": peak, "unit": "GB/s",
+                  "frac": it_bytes / (t_tik / niter) / 1e9 / peak, "peak_kind": peak_kind,
+                  "algorithmic_bytes_per_iteration": it_bytes, "traffic": None},
+        e2e={"value": niter / t_e2e, "unit": "iter/s",
+             "h2d_bytes_per_step": sum(p["pixels"].nbytes for p in probs) / niter,
+             "d2h_bytes_per_step": 4.0 * V / niter,
+             "call": "parallelbeam.alg.reconstruct_batched('cgls_tikhonov', 64 problems)"},
+        clocks=clk, cpu_baseline=cpu)))
+
+
+def uneven_cpu_sample(probs):
+    """The reference's own cgls_tikhonov on 4 of the 64 problems, t(2
+    iterations) - t(1), scaled to 40 iterations of all 64 by their share of
+    voxels x angles."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.reference_available():
+        return None
+    threads = os.cpu_count() or 1
+    sel = [0, 16, 32, 48]
+    work = lambda p: p["pixels"].shape[0] * p["pixels"].shape[1] * p["pixels"].shape[2] ** 2  # noqa
+    t_sel = 0.0
+    for i in sel:
+        p = probs[i]
+        times = []
+        for it in (1, 2):
+            t0 = time.perf_counter()
+            with O.quiet():
+                O.ref_pb_reconstruct(3, p["pixels"], p["deg"], 0.0, 1, it, True, lam=p["lam"],
+                                     nthreads=threads)
+            times.append(time.perf_counter() - t0)
+        t_sel += max(times[1] - times[0], 1e-9)
+    scale = sum(work(p) for p in probs) / sum(work(probs[i]) for i in sel)
+    t_batch_iter = t_sel * scale
+    return {"value": 1.0 / t_batch_iter, "unit": "iter/s", "cores": threads, "kind": "reference",
+            "sample": "reference cgls_tikhonov on problems 0, 16, 32, 48; t(2 iter) - t(1 iter), "
+                      "scaled to all 64 by n_angles x n_v x n_h^2"}
+
+
+def run_autograd(args):
+    """Differentiable cone projector: 8 volumes of 256^3 seeded ellipsoids
+    (2 mm voxels), 360 angles over [0, 2 pi), 384 x 384 detector of 1.6 mm
+    pixels, source/detector 500 mm; loss ||A x - y||^2 against noisy
+    sinograms, minimised by Adam.  A step is one Adam step over the batch
+    (8 forward and 8 back projections)."""
+    import numpy as np
+    import torch
+
+    from ccpi.reconstruction.autograd import Projector
+    from ccpi.reconstruction.device import cone_plan
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n, na, nd, nb = 256, 360, 384, 8
+    plan = cone_plan(n, 2.0, na, nd, 1.6, 500.0, 500.0)
+    A = Projector(plan)
+    xt = torch.stack([ellipsoids(torch, dev, n, 40, (5.0, 60.0), seed=50 + b) for b in range(nb)])
+    with torch.no_grad():
+        y = A(xt)
+        gen = torch.Generator(device=dev).manual_seed(5)
+        y += 0.01 * float(y.abs().max()) * torch.randn(y.shape, device=dev, generator=gen)
+    x = torch.zeros_like(xt, requires_grad=True)
+    opt = torch.optim.Adam([x], lr=0.02)
+
+    def step():
+        opt.zero_grad()
+        r = A(x) - y
+        loss = (r * r).sum()
+        loss.backward()
+        opt.step()
+        return loss
+    l0 = float(step().detach())
+    for _ in range(max(args.warmup - 1, 0)):
+        step()
+    clocks = Clocks(0)
+    t = cuda_time(torch, step, args.steps)
+    clk = clocks.stop()
+    l1 = float(step().detach())
+    # checks at full size on one volume: dot test and central differences
+    with torch.no_grad():
+        g = torch.Generator(device=dev).manual_seed(9)
+        u = torch.rand((n, n, n), device=dev, generator=g)
+        w = torch.rand(plan.sino_shape, device=dev, generator=g)
+        lhs = float((plan.forward(u).double() * w.double()).sum())
+        rhs = float((u.double() * plan.backward(w).double()).sum())
+    P = na * nd * nd
+    t_fp = cuda_time(torch, lambda: plan.forward(u), 2)
+    t_bp = cuda_time(torch, lambda: plan.backward(w), 2)
+    print(json.dumps(line_common(
+        args, "differentiable cone projector: 8 x 256^3 ellipsoid volumes, 360 angles over "
+              "2 pi, 384^2 detector at 1.6 mm, 2 mm voxels, source/detector 500 mm, Adam on "
+              "||Ax - y||^2", 1.0 / t, "step/s", t,
+        {"batch": nb, "grid": [n, n, n], "angles": na, "detector": [nd, nd]},
+        fp_ms=1000 * t_fp, bp_ms=1000 * t_bp,
+        projector_rays_per_s={"forward": P / t_fp, "backward": P / t_bp},
+        loss_first=l0, loss_after=l1, dot_test_rel=abs(lhs - rhs) / abs(lhs),
+        gpu_launches=2 * nb * args.steps, clocks=clk)))
+
+
 # -------------------------------------------------------------------- main
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "sirt":
+        return {"cone-cgls": run_cone_cgls, "uneven": run_uneven,
+                "autograd": run_autograd}[args.workload](args)
     import ctypes
 
     import numpy as np

@@ -76,6 +76,25 @@ int ccpi_version(void);
 int ccpi_pb_grid(int n_angles, int n_v, int n_h, double rotation_centre,
                  int pixels_per_voxel, int dims[5]);
 
+/* The explicit geometry ccpi_pb_reconstruct derives from a sinogram shape
+ * (the same front-end as ccpi_pb_grid: Core/src/diamond.cpp:35-86,
+ * :479-501), for callers that keep their data on the device and use
+ * ccpi_plan_create.  The caller provides angles_rad (n_angles),
+ * h_pixels (n_h) and v_pixels (n_v_padded from ccpi_pb_grid); `geometry`
+ * is filled and points into them. */
+int ccpi_pb_geometry(int n_angles, int n_v, int n_h, const float *angles_deg,
+                     double rotation_centre, int pixels_per_voxel,
+                     double *angles_rad, double *h_pixels, double *v_pixels,
+                     ccpi_geometry *geometry);
+
+/* Device-side layout change of a parallel-beam sinogram: numpy layout
+ * (n_angles, n_v, n_h) -> (n_angles, n_h, n_v_padded) with the data in
+ * rows [v_offset, v_offset + n_v) and zeros elsewhere, as the reference's
+ * Diamond::read_scans stores it (Core/src/diamond.cpp:394-451).
+ * Asynchronous on `stream`. */
+int ccpi_pb_pack(const float *d_pixels, int n_angles, int n_v, int n_h,
+                 int n_v_padded, int v_offset, float *d_sino, void *stream);
+
 /* parallelbeam.alg.{cgls,sirt,mlem,cgls_conv,cgls_tikhonov,cgls_TVreg}
  * and their *_step forms.  Replaces reconstruct_iter
  * (Wrappers/Python/src/diamond_wrapper.cpp:53-137; *_step: :140-257).
