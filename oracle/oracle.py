@@ -313,14 +313,24 @@ def ref_pb_reconstruct(alg, pixels, angles_deg, cor, ppv, niter, is_log, lam=0.0
     na, nv, nh = pixels.shape
     dims, _ = ref_pb_geometry(na, nv, nh, cor, ppv)
     out = np.zeros(tuple(dims[:3]), np.float32)
+    # cgls_regularize::reconstruct updates r_vox (a volume) with sinogram
+    # extents (Core/src/Algorithms/cgls.cpp:386): pad every allocation by
+    # the overrun ratio so that those writes land in padding
+    n_vox = int(dims[0]) * int(dims[1]) * int(dims[2])
+    n_pix = na * nh * int(dims[3])
+    pad = max(0.0, n_pix / max(n_vox, 1) - 1.0) + 0.05 if alg in (3, 4) else 0.0
     x0p = None
     if x0 is not None:
         x0 = np.ascontiguousarray(x0, np.float32)
         x0p = x0.ctypes.data
-    rc = reference().ref_pb_reconstruct(alg, pixels, na, nv, nh,
-                                        np.ascontiguousarray(angles_deg, np.float32), float(cor),
-                                        ppv, niter, nthreads, int(bool(is_log)), float(lam), x0p,
-                                        out)
+    reference().ref_set_pad_factor(pad)
+    try:
+        rc = reference().ref_pb_reconstruct(alg, pixels, na, nv, nh,
+                                            np.ascontiguousarray(angles_deg, np.float32),
+                                            float(cor), ppv, niter, nthreads, int(bool(is_log)),
+                                            float(lam), x0p, out)
+    finally:
+        reference().ref_set_pad_factor(0.0)
     if rc:
         raise RuntimeError(f"reference reconstruct failed ({rc})")
     return out
