@@ -67,6 +67,18 @@ def parse():
     return args
 
 
+def load_traffic():
+    """DRAM bytes per launch of the dominant kernel on this workload, from
+    one ncu capture of the same command (1-pass metrics, full size)."""
+    if globals().get("NH") != 768:
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "pb_traffic_768x768x256.json")) as f:
+            return float(json.load(f)["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -802,7 +814,8 @@ def main():
             "plain_sample": plain["sample"] if plain else None,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": alg_bytes, "traffic": None},
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "traffic": load_traffic()},
             "e2e": {"value": world * e2e_it / t_e2e, "unit": "iter/s",
                     "h2d_bytes_per_step": host_in.numel() * 4 / e2e_it,
                     "d2h_bytes_per_step": host_out.numel() * 4 / e2e_it,
