@@ -797,13 +797,13 @@ __device__ void pb_bp_stage(const Geom &g, int tx0, int ty0, int tw, int th, int
 }
 
 // Vector over z (row v == slice z): each thread owns NP (column, group)
-// pairs of VW = 8 (two float4) or 4 slices; groups are the fastest index so
+// pairs of VW = 16, 8 or 4 slices (four, two or one float4); groups are the fastest index so
 // the lanes of a warp share a column and read its staged rays as
 // broadcasts.  Group k holds float4 k, k + nzg, ... of the column (nzg =
 // nz / VW groups), so each load instruction of a warp covers one contiguous
 // 512-byte run of the sinogram row.
 template <int NP, int VW, int EPI>
-__global__ void __launch_bounds__(256, NP <= 2 ? 4 : (NP <= 4 ? 2 : 1)) pb_bp_vec(Geom g, const float *__restrict__ pix,
+__global__ void __launch_bounds__(256, NP * VW <= 16 ? 4 : (NP * VW <= 32 ? 2 : 1)) pb_bp_vec(Geom g, const float *__restrict__ pix,
                                                  float *__restrict__ vol, Epi e, int tw, int th,
                                                  int *err) {
   extern __shared__ BpEntry ent[];
@@ -982,6 +982,10 @@ int launch_fp(const Geom &g, const float *vol, float *pix, const Epi &e, int gri
   return 0;
 }
 
+#ifndef PB_BP_VW16
+#define PB_BP_VW16 1 // 16 slices per (column, group) pair when nz % 16 == 0
+#endif
+
 // Column tile and pairs per thread for the back projector: enough
 // (column, slice group) pairs to fill 256 threads, at most 16 per thread.
 struct BpShape {
@@ -992,7 +996,9 @@ BpShape bp_shape(const Geom &g) {
   BpShape b;
   b.vw = 1;
   if (g.map_type == 1 && g.nv == g.nz) {
-    if (g.nz % 8 == 0)
+    if (PB_BP_VW16 && g.nz % 16 == 0)
+      b.vw = 16;
+    else if (g.nz % 8 == 0)
       b.vw = 8;
     else if (g.nz % 4 == 0)
       b.vw = 4;
@@ -1005,7 +1011,7 @@ BpShape bp_shape(const Geom &g) {
     b.th = 8;
   }
   b.np = (b.tw * b.th * per_col + 255) / 256;
-  while (b.np > (b.vw == 8 ? 8 : 16) && b.tw * b.th > 1) {
+  while (b.np > (b.vw >= 8 ? 8 : 16) && b.tw * b.th > 1) {
     if (b.tw >= b.th)
       b.tw = (b.tw + 1) / 2;
     else
@@ -1020,7 +1026,9 @@ int launch_bp_np(const Geom &g, const BpShape &b, const float *pix, float *vol, 
                  int *err, cudaStream_t st) {
   const int tiles = ((g.nx + b.tw - 1) / b.tw) * ((g.ny + b.th - 1) / b.th);
   const size_t smem = sizeof(BpEntry) * b.tw * b.th * kBpAngles;
-  if (b.vw == 8)
+  if (b.vw == 16)
+    pb_bp_vec<NP, 16, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
+  else if (b.vw == 8)
     pb_bp_vec<NP, 8, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
   else if (b.vw == 4)
     pb_bp_vec<NP, 4, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
@@ -1043,7 +1051,7 @@ int launch_bp(const Geom &g, const float *pix, float *vol, const Epi &e, int *er
     return launch_bp_np<EPI, 4>(g, b, pix, vol, e, err, st);
   if (b.np <= 8)
     return launch_bp_np<EPI, 8>(g, b, pix, vol, e, err, st);
-  if (b.vw == 8)
+  if (b.vw >= 8)
     return 2;
   return launch_bp_np<EPI, 16>(g, b, pix, vol, e, err, st);
 }
