@@ -803,7 +803,7 @@ __device__ void pb_bp_stage(const Geom &g, int tx0, int ty0, int tw, int th, int
 // nz / VW groups), so each load instruction of a warp covers one contiguous
 // 512-byte run of the sinogram row.
 template <int NP, int VW, int EPI>
-__global__ void __launch_bounds__(256, NP * VW <= 16 ? 4 : (NP * VW <= 32 ? 2 : 1)) pb_bp_vec(Geom g, const float *__restrict__ pix,
+__global__ void __launch_bounds__(256, NP * VW <= 16 ? 4 : (NP * VW <= 32 ? 3 : 1)) pb_bp_vec(Geom g, const float *__restrict__ pix,
                                                  float *__restrict__ vol, Epi e, int tw, int th,
                                                  int *err) {
   extern __shared__ BpEntry ent[];
@@ -985,6 +985,9 @@ int launch_fp(const Geom &g, const float *vol, float *pix, const Epi &e, int gri
 #ifndef PB_BP_VW16
 #define PB_BP_VW16 1 // 16 slices per (column, group) pair when nz % 16 == 0
 #endif
+#ifndef PB_BP_VW32
+#define PB_BP_VW32 0 // 32 slices per pair when nz % 32 == 0
+#endif
 
 // Column tile and pairs per thread for the back projector: enough
 // (column, slice group) pairs to fill 256 threads, at most 16 per thread.
@@ -996,7 +999,9 @@ BpShape bp_shape(const Geom &g) {
   BpShape b;
   b.vw = 1;
   if (g.map_type == 1 && g.nv == g.nz) {
-    if (PB_BP_VW16 && g.nz % 16 == 0)
+    if (PB_BP_VW32 && g.nz % 32 == 0)
+      b.vw = 32;
+    else if (PB_BP_VW16 && g.nz % 16 == 0)
       b.vw = 16;
     else if (g.nz % 8 == 0)
       b.vw = 8;
@@ -1008,7 +1013,7 @@ BpShape bp_shape(const Geom &g) {
   b.th = 4;
   if (per_col * 16 < 256) {
     b.tw = 8;
-    b.th = 8;
+    b.th = per_col * 32 >= 256 ? 4 : 8;
   }
   b.np = (b.tw * b.th * per_col + 255) / 256;
   while (b.np > (b.vw >= 8 ? 8 : 16) && b.tw * b.th > 1) {
@@ -1026,7 +1031,10 @@ int launch_bp_np(const Geom &g, const BpShape &b, const float *pix, float *vol, 
                  int *err, cudaStream_t st) {
   const int tiles = ((g.nx + b.tw - 1) / b.tw) * ((g.ny + b.th - 1) / b.th);
   const size_t smem = sizeof(BpEntry) * b.tw * b.th * kBpAngles;
-  if (b.vw == 16)
+  if (PB_BP_VW32 && b.vw == 32)
+    pb_bp_vec<NP, PB_BP_VW32 ? 32 : 16, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw,
+                                                                        b.th, err);
+  else if (b.vw == 16)
     pb_bp_vec<NP, 16, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
   else if (b.vw == 8)
     pb_bp_vec<NP, 8, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
