@@ -266,12 +266,15 @@ __device__ __forceinline__ float fp_epilogue(float acc, i64 idx, const Epi &e, d
   return acc;
 }
 
+// One FP64 partial sum of squares per CTA.  A forward projection of more
+// than 256 rows runs as several launches over row ranges on one stream with
+// the same grid: the first (add == false) stores, the later ones add.
 template <int NWARPS>
-__device__ void store_partial(double ssq, const Epi &e) {
+__device__ void store_partial(double ssq, const Epi &e, bool add = false) {
   __shared__ double red[NWARPS];
   const double t = cta_sum<NWARPS>(ssq, red);
   if (threadIdx.x == 0)
-    e.partials[blockIdx.x] = t;
+    e.partials[blockIdx.x] = add ? e.partials[blockIdx.x] + t : t;
 }
 
 // Staged cell lists: the warp-uniform walk emits (column, length) pairs into
@@ -597,7 +600,7 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
     }
   }
   if (EPI == EPI_NORM)
-    store_partial<kLaneWarps>(ssq, e);
+    store_partial<kLaneWarps>(ssq, e, v0 > 0);
 }
 
 // ---- forward, any row->slice mapping (p2D.cpp:63-213 cases 2, 4, default)
@@ -664,7 +667,7 @@ __global__ void __launch_bounds__(kFpWarps * 32) pb_fp_scalar(Geom g, const floa
     }
   }
   if (EPI == EPI_NORM)
-    store_partial<kFpWarps>(ssq, e);
+    store_partial<kFpWarps>(ssq, e, v0 > 0);
 }
 
 // ---- backward

@@ -214,3 +214,21 @@ def test_device_api_plan_equals_host_call(alg, cuda):
     x = torch.zeros(plan.shape, device=cuda)
     plan.solve(alg, sino, x, 5)
     assert np.array_equal(x.cpu().numpy(), host)
+
+
+def test_cgls_more_rows_than_one_projector_pass(cuda):
+    """A parallel-beam problem of more than 256 detector rows (the forward
+    projector then runs in several row passes): CGLS against the FP64
+    oracle, whose step scalars use every row."""
+    import torch
+    from ccpi.reconstruction.device import parallel_plan
+    rng = np.random.default_rng(41)
+    shape, na, nh = (20, 20, 300), 16, 30
+    p = parallel_plan(shape, na, nh)
+    x_true = rng.random(shape).astype(np.float32)
+    sino = p.forward(torch.from_numpy(x_true).to(cuda))
+    x = torch.zeros(shape, device=cuda)
+    p.solve(0, sino, x, 3)
+    g = O.parallel_geometry(shape, na, nh)
+    r64 = O.solve(g, 0, sino.cpu().numpy().astype(np.float64), 3, fp64=True)
+    assert rel_l2(x.cpu().numpy(), r64) <= 1e-4
