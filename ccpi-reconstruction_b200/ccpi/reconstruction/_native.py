@@ -51,6 +51,10 @@ def _load():
     lib.ccpi_pb_reconstruct_batched.argtypes = [_c_int, _c_int, P(_vp), _i32p, _i32p, _i32p,
                                                 P(_vp), _f64p, _c_int, _c_int, _c_int, _vp,
                                                 P(_vp)]
+    lib.ccpi_pb_aml_ring_artefacts.argtypes = [_f32p, _c_int, _c_int, _c_int, ctypes.c_float,
+                                               ctypes.c_float, _c_int, _f32p]
+    lib.ccpi_ring_filter_aml.argtypes = [_vp, _c_int, _c_int, _c_int, _c_dbl, _c_dbl, _c_int,
+                                         _vp]
     lib.ccpi_pb_forward_project.argtypes = [_f32p, _c_int, _c_int, _c_int, _f32p, _c_int,
                                             _c_int, _vp, _i32p]
     lib.ccpi_pb_backward_project.argtypes = [_f32p, _c_int, _c_int, _c_int, _f32p, _c_dbl,

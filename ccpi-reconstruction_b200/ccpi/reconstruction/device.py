@@ -223,3 +223,19 @@ def pack_parallel(pixels, n_v_padded, v_offset, out=None):
                                ctypes.c_void_p(torch.cuda.current_stream(pixels.device).cuda_stream)),
             "ccpi_pb_pack")
     return out
+
+
+def ring_filter_aml(sino, param_n, param_r, num_series):
+    """AML ring-artefact filter (``ccpi_ring_filter_aml``) on a log sinogram
+    in the internal layout (n_angles, n_h, n_v), in place, on torch's
+    current stream; returns sino."""
+    if not (sino.is_cuda and sino.dtype == torch.float32 and sino.is_contiguous()
+            and sino.dim() == 3):
+        raise ValueError("sinogram must be a contiguous 3-D float32 CUDA tensor")
+    na, nh, nv = sino.shape
+    N.check(N.lib.ccpi_ring_filter_aml(ctypes.c_void_p(sino.data_ptr()), na, nh, nv,
+                                       float(param_n), float(param_r), int(num_series),
+                                       ctypes.c_void_p(
+                                           torch.cuda.current_stream(sino.device).cuda_stream)),
+            "ccpi_ring_filter_aml")
+    return sino

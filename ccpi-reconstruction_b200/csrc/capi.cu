@@ -508,6 +508,47 @@ int ccpi_pb_reconstruct_batched(int n, int alg, const float *const *pixels, cons
   return 0;
 }
 
+int ccpi_pb_aml_ring_artefacts(const float *pixels, int na, int nv, int nh, float param_n,
+                               float param_r, int num_series, float *out) {
+  ccpi::g_last_error.clear();
+  if (!pixels || !out || na < 1 || nv < 1 || nh < 2) {
+    set_error("ccpi_pb_aml_ring_artefacts: need pixels (n_angles >= 1, n_v >= 1, n_h >= 2) "
+              "and an output buffer");
+    return 1;
+  }
+  const i64 n = i64(na) * nv * nh;
+  // p = -log(pixels) with the C library's logf (diamond_wrapper.cpp:28-34)
+  std::vector<float> logged(size_t(n), 0.0f);
+  neglog_host(pixels, logged.data(), n);
+  DevBuf raw, sino;
+  if (!raw.alloc(n * 4) || !sino.alloc(n * 4))
+    return 2;
+  cudaStream_t st = 0;
+  if (!ccpi::cuda_ok(cudaMemcpy(raw.p, logged.data(), n * 4, cudaMemcpyHostToDevice),
+                     "upload pixels"))
+    return 2;
+  ccpi::k_pack_parallel(raw.f(), sino.f(), na, nv, nh, nv, 0, st); // -> [a][h][v]
+  const int rc = ccpi::aml_ring_filter(sino.f(), na, nh, nv, param_n, param_r, num_series, st);
+  if (rc)
+    return rc;
+  ccpi::k_unpack_parallel(sino.f(), raw.f(), na, nh, nv, st); // -> [a][v][h]
+  if (!ccpi::cuda_ok(cudaMemcpy(logged.data(), raw.p, n * 4, cudaMemcpyDeviceToHost),
+                     "download pixels"))
+    return 2;
+  // back to transmission with the C library's expf (diamond_wrapper.cpp:45-48)
+#pragma omp parallel for schedule(static)
+  for (i64 i = 0; i < n; i++)
+    out[i] = std::exp(-logged[size_t(i)]);
+  return 0;
+}
+
+int ccpi_ring_filter_aml(float *d_sino, int n_angles, int n_h, int n_v, double param_n,
+                         double param_r, int num_series, void *stream) {
+  ccpi::g_last_error.clear();
+  return ccpi::aml_ring_filter(d_sino, n_angles, n_h, n_v, param_n, param_r, num_series,
+                               cudaStream_t(stream));
+}
+
 int ccpi_pb_forward_project(const float *volume, int vx, int vy, int vz, const float *angles_deg,
                             int na, int ppv, float *out, int out_dims[3]) {
   ccpi::g_last_error.clear();

@@ -40,5 +40,9 @@ int session_finish(void *s, double *h_norms);
 void session_destroy(void *s);
 int solve_batched(int n, const ccpi_plan *const *plans, int alg, const float *const *sino,
                   float *const *x, int niter, const double *lambda, cudaStream_t st);
+// AML ring-artefact filter on a device sinogram [angle][h][v], in place
+// (aml.cu); synchronises st.
+int aml_ring_filter(float *d_sino, int na, int nh, int nv, double param_n, double param_r,
+                    int num_series, cudaStream_t st);
 
 } // namespace ccpi

@@ -126,6 +126,23 @@ int ccpi_pb_reconstruct_batched(int n, int alg, const float *const *pixels,
                                 int is_pixels_in_log, const double *regularize,
                                 float *const *volumes);
 
+/* parallelbeam.filters.aml_ring_artefacts: the AML ring-artefact filter
+ * (Wrappers/Python/src/diamond_wrapper.cpp:18-51 over
+ * CCPi::remove_aml_ring_artefacts, Core/src/diamond.cpp:660-808).
+ * pixels and out: (n_angles, n_v, n_h) transmission data; the filter runs
+ * on -log(pixels) and out = exp(-filtered).  Parameters the reference
+ * rejects (param_n < 0, param_r <= 0, num_series outside [1, 100]) are
+ * errors. */
+int ccpi_pb_aml_ring_artefacts(const float *pixels, int n_angles, int n_v,
+                               int n_h, float param_n, float param_r,
+                               int num_series, float *out);
+
+/* The same filter on a device log sinogram in the internal layout
+ * (n_angles, n_h, n_v), in place, on `stream` (the call waits for it). */
+int ccpi_ring_filter_aml(float *d_sino, int n_angles, int n_h, int n_v,
+                         double param_n, double param_r, int num_series,
+                         void *stream);
+
 /* parallelbeam.alg.pb_forward_project (diamond_wrapper.cpp:421-556):
  * volume (vx, vy, vz) -> (n_angles, n_v_padded, max(vx, vy)).  With
  * out == NULL only out_dims is filled. */

@@ -102,6 +102,7 @@ def restate():
             fn.restype = _c_int
             getattr(lib, f"rs_regularize_{suf}").argtypes = [_c_int, _c_int, _c_int, _c_int, p, p]
         lib.rs_neglog_f32.argtypes = [_f32p, _f32p, ctypes.c_longlong]
+        lib.rs_aml_ring_f32.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_dbl, _c_dbl, _c_int]
         _rs = lib
     return _rs
 
@@ -263,6 +264,9 @@ def reference():
         lib.ref_cb_reconstruct.argtypes = [_c_int, _f32p, _c_int, _c_int, _c_int, _f32p,
                                            _c_int] + [_c_dbl] * 5 + [_c_int, _c_int, _c_int,
                                                                      _c_dbl, _f32p]
+        lib.ref_aml_ring.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_dbl, _c_dbl, _c_int]
+        lib.ref_aml_ring_artefacts.argtypes = [_f32p, _c_int, _c_int, _c_int, ctypes.c_float,
+                                               ctypes.c_float, _c_int, _f32p]
         lib.ref_cb_solve_explicit.argtypes = [_c_int] + [_c_dbl] * 4 + [
             _f64p, _c_int, _f64p, _c_int, _f64p, _c_int, _f32p, _f64p, _f64p, _c_int, _c_int,
             _c_int, _c_int, _c_dbl, _c_int, _f32p]
@@ -431,3 +435,38 @@ def parallel_geometry(shape, n_angles, nh, nv=None, cor_shift=0.0, span=math.pi)
     v = np.arange(nv, dtype=np.float64) - (nv - 1) / 2.0
     return Geometry(0, ang, h, v, (-nx / 2.0, -ny / 2.0, -nz / 2.0), (1.0, 1.0, 1.0),
                     (nx, ny, nz))
+
+
+# ------------------------------------------------------- AML ring filter
+def aml_ring(p, param_n, param_r, num_series):
+    """The restatement's AML ring filter on a log sinogram (na, nh, nv);
+    returns the filtered copy (Core/src/diamond.cpp:660-808)."""
+    lib = restate()
+    out = np.array(p, np.float32, order="C")
+    na, nh, nv = out.shape
+    rc = lib.rs_aml_ring_f32(out, na, nh, nv, float(param_n), float(param_r), int(num_series))
+    if rc:
+        raise ValueError("AML ring filter: parameters out of range")
+    return out
+
+
+def ref_aml_ring(p, param_n, param_r, num_series):
+    """The reference's remove_aml_ring_artefacts on a log sinogram (na, nh, nv)."""
+    out = np.array(p, np.float32, order="C")
+    na, nh, nv = out.shape
+    with quiet():
+        reference().ref_aml_ring(out, na, nh, nv, float(param_n), float(param_r),
+                                 int(num_series))
+    return out
+
+
+def ref_aml_ring_artefacts(pixels, param_n, param_r, num_series):
+    """parallelbeam.filters.aml_ring_artefacts as the reference's wrapper
+    computes it: (na, nv, nh) transmission in and out."""
+    pixels = np.ascontiguousarray(pixels, np.float32)
+    na, nv, nh = pixels.shape
+    out = np.zeros_like(pixels)
+    with quiet():
+        reference().ref_aml_ring_artefacts(pixels, na, nv, nh, float(param_n), float(param_r),
+                                           int(num_series), out)
+    return out

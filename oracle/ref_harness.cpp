@@ -14,6 +14,7 @@
 //    (Core/src/Algorithms/cgls.cpp:386), out of bounds when n_angles > nx.
 // Both only write memory that is never read back for the result, so every
 // allocation made by the reference is padded (operator new below).
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -484,4 +485,32 @@ extern "C" void ref_regularize(int alg, int nx, int ny, int nz, const float *a,
   else
     CCPi::tv_regularize(out, in, nx, ny, nz);
   std::memcpy(b, out.data(), sizeof(float) * std::size_t(nx) * ny * nz);
+}
+
+// The reference's AML ring-artefact filter (CCPi::remove_aml_ring_artefacts,
+// Core/src/diamond.cpp:660-808) on a log sinogram in its pixel layout
+// [angle][h][v], in place.
+extern "C" void ref_aml_ring(float *p, int na, int nh, int nv, double param_n, double param_r,
+                             int num_series) {
+  pixel_data px(boost::extents[na][nh][nv]);
+  std::memcpy(px.data(), p, sizeof(float) * std::size_t(na) * nh * nv);
+  CCPi::remove_aml_ring_artefacts(px, na, nh, nv, param_n, param_r, num_series);
+  std::memcpy(p, px.data(), sizeof(float) * std::size_t(na) * nh * nv);
+}
+
+// parallelbeam.filters.aml_ring_artefacts as the reference's wrapper runs it
+// (Wrappers/Python/src/diamond_wrapper.cpp:18-51): pixels (na, nv, nh)
+// transmission in, exp(-filtered -log) out, same layout.
+extern "C" void ref_aml_ring_artefacts(const float *pixels, int na, int nv, int nh, float param_n,
+                                       float param_r, int num_series, float *out) {
+  pixel_3d p(boost::extents[na][nh][nv]);
+  for (int i = 0; i < na; i++)
+    for (int j = 0; j < nh; j++)
+      for (int k = 0; k < nv; k++)
+        p[i][j][k] = -std::log(pixels[(std::size_t(i) * nv + k) * nh + j]);
+  CCPi::remove_aml_ring_artefacts(p, na, nh, nv, param_n, param_r, num_series);
+  for (int i = 0; i < na; i++)
+    for (int j = 0; j < nv; j++)
+      for (int k = 0; k < nh; k++)
+        out[(std::size_t(i) * nv + j) * nh + k] = std::exp(-p[i][k][j]);
 }

@@ -1259,3 +1259,90 @@ void rs_neglog_f32(const float *in, float *out, long long n) {
     out[i] = -std::log(in[i]);
 }
 }
+
+// ---------------------------------------------------------------------------
+// AML ring-artefact filter (Core/src/diamond.cpp:660-808; Applied
+// Mathematics Letters 23, p1489).  For every detector row v and every term
+// s of the angular series (1, sqrt2 sin(k pi a / na), sqrt2 cos(k pi a / na)
+// for k < num_series): project the sinogram onto the term (FP64 sum over
+// angles in order), form the regularised second difference of that profile
+// along h, smooth it with the fixed matrix of the first series order
+// (diamond.cpp:775-781 uses that one matrix for every term), and subtract
+// the term back from every angle in float.  Series terms apply one after
+// another to the updated sinogram.
+extern "C" int rs_aml_ring_f32(float *p, int na, int nh, int nv, double param_n,
+                               double param_r, int num_series) {
+  if (param_n < -1e-10 || param_r < 1e-8 || num_series < 1 || num_series > 100)
+    return 1;
+  const int nx = nh;
+  const int nterms = 2 * num_series - 1;
+  // series table: term 0 is 1, terms 2k-1 / 2k are sqrt2 sin / sqrt2 cos
+  std::vector<double> term(size_t(nterms) * na, 1.0);
+  const double r2 = std::sqrt(2.0);
+  for (int k = 1; k < num_series; k++) {
+    const double slope = double(k) * M_PI / double(na);
+    for (int a = 0; a < na; a++) {
+      const double x = double(a) * slope;
+      double sv = std::sin(x), cv = std::cos(x);
+      sv *= r2;
+      cv *= r2;
+      term[size_t(2 * k - 1) * na + a] = sv;
+      term[size_t(2 * k) * na + a] = cv;
+    }
+  }
+  // smoothing matrix of order 1
+  const double alpha = (param_n + param_r) * 1.0;
+  const double mdiv = std::sqrt(alpha * (alpha + 4.0));
+  const double tau = 2.0 * std::asinh(std::sqrt(alpha) / 2.0);
+  std::vector<double> ex(size_t(2 * nx + 2));
+  for (int i = 0; i < 2 * nx + 2; i++)
+    ex[i] = std::exp(-tau * double(i));
+  const double dv = mdiv * (1.0 - ex[2 * nx]);
+  std::vector<double> mat(size_t(nx) * nx);
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < nx; j++) {
+      const int lo = std::min(i, j) + 1, hi = std::max(i, j) + 1;
+      double m = ex[hi - lo] * (1.0 + ex[2 * nx - 2 * hi + 1]) * (1.0 + ex[2 * lo - 1]);
+      m /= dv;
+      mat[size_t(i) * nx + j] = m;
+    }
+  std::vector<double> prof(nx), diff(nx);
+  std::vector<float> corr(nx);
+  for (int v = 0; v < nv; v++) {
+    for (int t = 0; t < nterms; t++) {
+      const double *w = term.data() + size_t(t) * na;
+      const int order = (t + 2) / 2;
+      for (int h = 0; h < nx; h++) {
+        double acc = 0.0;
+        for (int a = 0; a < na; a++)
+          acc += double(p[(size_t(a) * nh + h) * nv + v]) * w[a];
+        prof[h] = acc / double(na);
+      }
+      const double coef = param_n * double(order * order);
+      for (int h = 0; h < nx; h++) {
+        double d = coef * prof[h];
+        if (h < nx - 1) {
+          d += prof[h];
+          d -= prof[h + 1];
+        }
+        if (h >= 1) {
+          d += prof[h];
+          d -= prof[h - 1];
+        }
+        diff[h] = d;
+      }
+      for (int i = 0; i < nx; i++) {
+        double dp = 0.0;
+        for (int h = 0; h < nx; h++)
+          dp += diff[h] * mat[size_t(i) * nx + h];
+        corr[i] = float(dp);
+      }
+      for (int a = 0; a < na; a++) {
+        const float wf = float(w[a]);
+        for (int h = 0; h < nx; h++)
+          p[(size_t(a) * nh + h) * nv + v] -= wf * corr[h];
+      }
+    }
+  }
+  return 0;
+}

@@ -57,6 +57,12 @@ void rs_regularize_f32(int alg, int nx, int ny, int nz, const float *a,
 void rs_regularize_f64(int alg, int nx, int ny, int nz, const double *a,
                        double *b);
 
+/* AML ring-artefact filter (Core/src/diamond.cpp:660-808) on a log
+ * sinogram in the layout [angle][h][v], in place.  Returns 1 (and leaves p
+ * unchanged) for parameters the reference rejects. */
+int rs_aml_ring_f32(float *p, int na, int nh, int nv, double param_n,
+                    double param_r, int num_series);
+
 /* -log(p) with the C library's logf, as the reference's read_scans does. */
 void rs_neglog_f32(const float *in, float *out, long long n);
 

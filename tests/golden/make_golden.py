@@ -7,7 +7,7 @@ The reference has no golden vectors of its own (its Python tests only
 smoke-run), so these fixtures pin both the restatement in oracle/ and the
 CUDA path.  Regenerate with:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && python tests/golden/make_golden.py [name-prefix ...]
 """
 from __future__ import annotations
 
@@ -38,7 +38,9 @@ def phantom2d(rng, n, nz, n_ell=6):
     return vol
 
 
-def main():
+def main(prefixes=()):
+    """Write every fixture, or only those whose names start with one of
+    `prefixes`."""
     os.makedirs(HERE, exist_ok=True)
     rng = np.random.default_rng(20240917)
     out = {}
@@ -158,11 +160,36 @@ def main():
                             px=np.array(px), mask_radius=np.array(6.5), dims=dims, geom=geo,
                             cgls3=crec)
 
+    out.update(aml_cases())
+    if prefixes:
+        out = {k: v for k, v in out.items() if k.startswith(tuple(prefixes))}
     for name, d in out.items():
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **d)
     total = sum(os.path.getsize(os.path.join(HERE, f"{n}.npz")) for n in out)
     print(f"wrote {len(out)} fixtures, {total / 1e6:.2f} MB")
 
 
+def aml_cases():
+    """parallelbeam.filters.aml_ring_artefacts on transmission stacks with
+    ring artefacts: a phantom projected by the reference, then per-column
+    gain errors (stripes in the sinogram, rings in the image)."""
+    rng = np.random.default_rng(515)
+    out = {}
+    for idx, (n, na, nh, nv, pn, pr, ns) in enumerate(
+            [(24, 60, 32, 3, 0.0, 0.005, 1), (32, 90, 44, 4, 0.2, 0.01, 3),
+             (20, 45, 30, 2, 1.0, 0.1, 2)]):
+        g = O.parallel_geometry((n, n, nv), na, nh)
+        vol = phantom2d(rng, n, nv) * 0.05
+        with O.quiet():
+            sino = O.ref_forward(g, vol)  # (na, nh, nv)
+        gains = 1.0 + 0.02 * rng.standard_normal((1, nh, nv))
+        trans = (np.exp(-sino.astype(np.float64)) * gains).astype(np.float32)
+        pixels = np.ascontiguousarray(trans.transpose(0, 2, 1))  # (na, nv, nh)
+        res = O.ref_aml_ring_artefacts(pixels, pn, pr, ns)
+        out[f"aml{idx}"] = dict(pixels=pixels, param_n=np.float32(pn), param_r=np.float32(pr),
+                                num_series=np.array(ns), out=res)
+    return out
+
+
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -107,3 +107,17 @@ def test_neglog_uses_float_log():
     p = np.array([0.5, 1.0, 0.25, 0.9999], np.float32)
     assert np.array_equal(O.neglog(p), -np.log(p).astype(np.float32)) or \
         max_rel(O.neglog(p), -np.log(p.astype(np.float64))) < 1e-7
+
+
+@pytest.mark.parametrize("name", golden_names("aml"))
+def test_aml_restatement_equals_reference(name):
+    """The restatement of the AML ring filter equals the reference's
+    remove_aml_ring_artefacts bit for bit, and the fixture is the reference
+    wrapper's output."""
+    if not O.reference_available():
+        pytest.skip("reference library not built")
+    d = golden(name)
+    pn, pr, ns = float(d["param_n"]), float(d["param_r"]), int(d["num_series"])
+    p = np.ascontiguousarray(O.neglog(d["pixels"]).transpose(0, 2, 1))  # (na, nh, nv)
+    assert np.array_equal(O.aml_ring(p, pn, pr, ns), O.ref_aml_ring(p, pn, pr, ns))
+    assert np.array_equal(O.ref_aml_ring_artefacts(d["pixels"], pn, pr, ns), d["out"])
