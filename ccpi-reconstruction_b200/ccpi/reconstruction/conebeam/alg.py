@@ -30,7 +30,8 @@ import numpy as np
 from .. import _native as N
 
 __all__ = ["cgls", "cgls_conv", "sirt", "mlem", "cgls_tikhonov", "cgls_TVreg",
-           "create_sinogram", "grid", "find_centre"]
+           "create_sinogram", "create_phantom", "create_phantom_volume", "grid",
+           "find_centre"]
 
 
 def grid(n_angles, n_h, n_v, pixels_per_voxel, source_to_sample, source_to_detector,
@@ -170,3 +171,74 @@ def create_sinogram(source_x, source_y, source_z, detector_x, h_pixels, v_pixels
     out = np.zeros((len(a), len(h), len(v)), np.float32)
     N.check(N.lib.ccpi_cb_create_sinogram(ctypes.byref(g), vol, out), "create_sinogram")
     return out
+
+
+# ---- demonstration phantom of the Nikon XTek instrument
+# (Nikon_XTek::create_phantom / build_phantom / initialise_phantom_volume,
+# Core/src/Readers/xtek.cpp:131-175, :392-457, :825-894; wrappers
+# conebeam_wrapper.cpp:238-310)
+_PH_PIXEL = 0.390625
+
+
+def _phantom_geometry():
+    """Source x, detector x, detector coordinates (512 columns = 512 rows),
+    250 angles in radians and the mask radius of the XTek phantom."""
+    source_x, detector_x = -250.0, 737.0
+    c = 0
+    while c < 1000 and not (-99.8046875 + float(c) * _PH_PIXEL >= 100.0 + 0.001):
+        c += 1
+    pix = -99.8046875 + np.arange(c, dtype=np.float64) * _PH_PIXEL
+    step = 2.0 * np.pi / 250.0
+    phi = np.arange(250, dtype=np.float64) * step
+    mask_radius = -source_x * np.sin(np.arctan(pix[-1] / (detector_x - source_x)))
+    return source_x, detector_x, pix, phi, float(mask_radius)
+
+
+def _phantom_volume(mask_radius):
+    """512^3 volume of three unit cubes and its voxel size / origin."""
+    n = 512
+    vsize = 2.0 * mask_radius / n
+    x = np.zeros((n, n, n), np.float32)
+    x[107:189, 107:189, 57:139] = 1.0
+    x[189:271, 189:271, 139:221] = 1.0
+    x[271:353, 271:353, 221:303] = 1.0
+    return x, vsize, -(vsize * n) / 2.0
+
+
+def create_phantom():
+    """(pixels (250, 512, 512) float32 projections, angles (250,) float32
+    degrees, source_x = 250.0, detector_x = 987.0, pixel_h_size,
+    pixel_v_size, mask_radius), as the reference returns them.  The
+    projections are this library's cone-beam forward projection of the
+    three-cube phantom; the reference projects it with its generic 3-D
+    Siddon routine (instrument::forward_project), which traces the same line
+    integrals with different float rounding."""
+    source_x, detector_x, pix, phi, mask_radius = _phantom_geometry()
+    vol, vsize, off = _phantom_volume(mask_radius)
+    g = N.Geometry()
+    g.kind = N.CONE
+    keep = [np.ascontiguousarray(phi), np.ascontiguousarray(pix), np.ascontiguousarray(pix)]
+    g.angles, g.h_pixels, g.v_pixels = (x.ctypes.data for x in keep)
+    g.n_angles, g.n_h, g.n_v = len(phi), len(pix), len(pix)
+    g.source = (ctypes.c_double * 3)(source_x, 0.0, 0.0)
+    g.detector_x = detector_x
+    g.origin = (ctypes.c_double * 3)(off, off, off)
+    g.voxel_size = (ctypes.c_double * 3)(vsize, vsize, vsize)
+    g.nx = g.ny = g.nz = vol.shape[0]
+    out = np.zeros((len(phi), len(pix), len(pix)), np.float32)
+    N.check(N.lib.ccpi_cb_create_sinogram(ctypes.byref(g), vol, out), "create_phantom")
+    angles = (phi * 180.0 / np.pi).astype(np.float32)
+    return (out, angles, -source_x, detector_x - source_x, _PH_PIXEL, _PH_PIXEL, mask_radius)
+
+
+def create_phantom_volume():
+    """(voxels (512, 512, 512) float32, angles (250,) float32 degrees,
+    h_pixels (512,) float32, v_pixels (512,) float32, source_x = 250.0,
+    detector_x = 987.0, pixel_h_size, pixel_v_size, mask_radius): the
+    phantom volume without projecting it, as the reference returns it."""
+    source_x, detector_x, pix, phi, mask_radius = _phantom_geometry()
+    vol, _, _ = _phantom_volume(mask_radius)
+    angles = (phi * 180.0 / np.pi).astype(np.float32)
+    p32 = pix.astype(np.float32)
+    return (vol, angles, p32, p32.copy(), -source_x, detector_x - source_x, _PH_PIXEL,
+            _PH_PIXEL, mask_radius)

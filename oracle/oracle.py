@@ -264,6 +264,7 @@ def reference():
         lib.ref_cb_reconstruct.argtypes = [_c_int, _f32p, _c_int, _c_int, _c_int, _f32p,
                                            _c_int] + [_c_dbl] * 5 + [_c_int, _c_int, _c_int,
                                                                      _c_dbl, _f32p]
+        lib.ref_cb_phantom_volume.argtypes = [_f32p, _f32p, _f32p, _f32p, _f64p]
         lib.ref_aml_ring.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_dbl, _c_dbl, _c_int]
         lib.ref_aml_ring_artefacts.argtypes = [_f32p, _c_int, _c_int, _c_int, ctypes.c_float,
                                                ctypes.c_float, _c_int, _f32p]
@@ -470,3 +471,17 @@ def ref_aml_ring_artefacts(pixels, param_n, param_r, num_series):
         reference().ref_aml_ring_artefacts(pixels, na, nv, nh, float(param_n), float(param_r),
                                            int(num_series), out)
     return out
+
+
+def ref_cb_phantom_volume():
+    """conebeam.create_phantom_volume from the reference: (vol, angles deg,
+    h_pixels, v_pixels, source_x, detector_x, pixel_h, pixel_v,
+    mask_radius)."""
+    vol = np.zeros((512, 512, 512), np.float32)
+    ang = np.zeros(250, np.float32)
+    h = np.zeros(512, np.float32)
+    v = np.zeros(512, np.float32)
+    sc = np.zeros(5, np.float64)
+    with quiet():
+        reference().ref_cb_phantom_volume(vol, ang, h, v, sc)
+    return (vol, ang, h, v) + tuple(float(x) for x in sc)

@@ -514,3 +514,31 @@ extern "C" void ref_aml_ring_artefacts(const float *pixels, int na, int nv, int 
       for (int k = 0; k < nh; k++)
         out[(std::size_t(i) * nv + j) * nh + k] = std::exp(-p[i][k][j]);
 }
+
+// conebeam.create_phantom_volume as the reference's wrapper builds it
+// (Wrappers/Python/src/conebeam_wrapper.cpp:270-310 over
+// Nikon_XTek::initialise_phantom_volume, Core/src/Readers/xtek.cpp:825-894):
+// vol (512^3), angles (250, degrees), h and v pixels (512 each) and
+// scalars {source_x, detector_x, pixel_h, pixel_v, mask_radius}.
+extern "C" void ref_cb_phantom_volume(float *vol, float *angles, float *h, float *v,
+                                      double *scalars) {
+  CCPi::Nikon_XTek *instrument = new CCPi::Nikon_XTek();
+  real_1d hp(512), vp(512);
+  voxel_data x = instrument->initialise_phantom_volume(hp, vp);
+  std::memcpy(vol, x.data(), sizeof(float) * std::size_t(512) * 512 * 512);
+  const double source_x = -1 * instrument->get_source_x();
+  const double detector_x = instrument->get_detector_x() + source_x;
+  real_1d phi = instrument->get_phi();
+  for (int i = 0; i < instrument->get_num_angles(); i++)
+    angles[i] = float(phi[i] * 180.0 / M_PI);
+  for (int i = 0; i < 512; i++) {
+    h[i] = float(hp[i]);
+    v[i] = float(vp[i]);
+  }
+  scalars[0] = source_x;
+  scalars[1] = detector_x;
+  scalars[2] = 0.390625;
+  scalars[3] = 0.390625;
+  scalars[4] = instrument->get_mask_radius();
+  delete instrument;
+}

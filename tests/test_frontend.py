@@ -100,3 +100,20 @@ def test_pb_geometry_matches_oracle_front_end(na, nv, nh, cor, ppv):
     assert np.array_equal(ang, og.angles) and np.array_equal(h, og.h_pixels)
     assert np.array_equal(v, og.v_pixels)
     assert tuple(g.origin) == tuple(og.origin) and tuple(g.voxel_size) == tuple(og.size)
+
+
+def test_create_phantom_volume_equals_reference():
+    """conebeam.create_phantom_volume: the reference's volume, angles,
+    detector coordinates and scalars, exactly (its test_conebeam.py:17-27
+    checks the same scalars of create_phantom)."""
+    import oracle as O
+    from ccpi.reconstruction.conebeam import alg
+    ours = alg.create_phantom_volume()
+    assert ours[1].shape == (250,) and ours[0].shape == (512, 512, 512)
+    assert ours[4:] == (250.0, 987.0, 0.390625, 0.390625, 25.151547886198443)
+    if not O.reference_available():
+        pytest.skip("reference library not built")
+    ref = O.ref_cb_phantom_volume()
+    for a, b in zip(ours[:4], ref[:4]):
+        assert a.dtype == b.dtype and np.array_equal(a, b)
+    assert ours[4:] == ref[4:]

@@ -150,3 +150,17 @@ def test_linearity_full_size_parallel(cuda):
     b2 = p.backward(a2)
     assert torch.equal(b2, 2 * b1)
     assert torch.isfinite(b1).all()
+
+
+def test_create_phantom_like_reference_test(cuda):
+    """conebeam.create_phantom returns what the reference's own test checks
+    (Wrappers/Python/test/test_conebeam.py:17-27), with finite, non-negative
+    projections of the three-cube phantom."""
+    from ccpi.reconstruction.conebeam import alg
+    data = alg.create_phantom()
+    assert data[0].shape == (250, 512, 512)
+    assert data[1].shape == (250,)
+    assert data[2] == 250.0 and data[3] == 987.0
+    assert data[4] == 0.390625 and data[5] == 0.390625
+    assert data[6] == 25.151547886198443
+    assert np.isfinite(data[0]).all() and data[0].min() >= 0.0 and data[0].max() > 0.0
