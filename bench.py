@@ -708,6 +708,21 @@ def main():
     sm.close()
     del xm
 
+    # ---- CGLS on the same problem, same form (FP64 step scalars)
+    xc = torch.zeros(plan.shape, device=dev)
+    sc = Session(plan, N.CGLS, sino, xc, args.warmup + args.steps)
+    sc.run(args.warmup)
+    torch.cuda.synchronize()
+    barrier()
+    e0.record(stream)
+    sc.run(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_cgls = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
+    sc.finish()
+    sc.close()
+    del xc
+
     # ---- dominant kernel: forward vs back projection, CUDA events
     tmp_p = torch.empty_like(sino)
     tmp_v = torch.empty(plan.shape, device=dev)
@@ -807,6 +822,7 @@ def main():
                        "l2": "inputs larger than L2 (sinogram 566 MB, volume 604 MB)",
                        "form": "batched: all slices per launch, one CUDA graph per iteration"},
             "mlem_iter_per_s": world * args.steps / t_mlem,
+            "cgls_iter_per_s": world * args.steps / t_cgls,
             "fp_ms": 1000.0 * t_fp, "bp_ms": 1000.0 * t_bp,
             "projector_rays_per_s": {"forward": rays, "backward": P / t_bp},
             "plain_iter_per_s": plain["iter_per_s"] if plain else None,
