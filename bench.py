@@ -494,6 +494,13 @@ def run_uneven(args):
         plan, nvp, voff = parallel_api_plan(na, nv, nh, p["deg"], 0.0, 1)
         plans.append(plan)
         sinos.append(pack_parallel(torch.from_numpy(p["pixels"]).to(dev), nvp, voff))
+    # the autotuner picks each plan's projector launch shapes
+    t0 = time.perf_counter()
+    tuned = [pl.autotune() for pl in plans]
+    t_tune = time.perf_counter() - t0
+    vw_counts = {}
+    for _, vw in tuned:
+        vw_counts[str(vw)] = vw_counts.get(str(vw), 0) + 1
     lams = [p["lam"] for p in probs]
     V = sum(int(np.prod(pl.shape)) for pl in plans)
     P = sum(int(np.prod(pl.sino_shape)) for pl in plans)
@@ -528,7 +535,8 @@ def run_uneven(args):
               "volumes, 90-900 angles, 1.5x detector columns, 2% noise), 40 iterations, all 64 "
               "in one graph per iteration", niter / t_tik, "iter/s", t_tik / niter,
         {"problems": len(probs), "voxels": V, "pixels": P, "iterations": niter,
-         "form": "batched: 64 problems per graph launch (16 branch streams)"},
+         "form": "batched: 64 problems per graph launch (16 branch streams)",
+         "autotune": {"seconds": t_tune, "bp_slices_per_lane_chosen": vw_counts}},
         tv_iter_per_s=niter / res["cgls_TVreg"]["batched_s"],
         plain_iter_per_s={k: niter / v["plain_s"] for k, v in res.items()},
         batched_over_plain={k: v["plain_s"] / v["batched_s"] for k, v in res.items()},

@@ -66,6 +66,7 @@ def _load():
         [_c_dbl] * 5 + [_c_int, _c_int, _c_int, _c_dbl, _vp, _f32p]
     lib.ccpi_cb_create_sinogram.argtypes = [P(Geometry), _f32p, _f32p]
     lib.ccpi_plan_create.argtypes = [P(Geometry), P(_vp)]
+    lib.ccpi_plan_autotune.argtypes = [_vp, _vp, _i32p]
     lib.ccpi_plan_destroy.argtypes = [_vp]
     lib.ccpi_plan_destroy.restype = None
     lib.ccpi_plan_voxels.argtypes = [_vp]

@@ -45,6 +45,17 @@ class Plan:
     def handle(self):
         return self._h
 
+    def autotune(self, device=None):
+        """Pick the fastest projector launch shapes for this plan
+        (``ccpi_plan_autotune``); call before solving.  Returns the choice
+        (grid or cone rows per lane, back projector slices per lane or 0)."""
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else device
+        chosen = np.zeros(2, np.int32)
+        N.check(N.lib.ccpi_plan_autotune(self._h,
+                                         ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream),
+                                         chosen), "ccpi_plan_autotune")
+        return int(chosen[0]), int(chosen[1])
+
     def close(self):
         if self._h:
             N.lib.ccpi_plan_destroy(self._h)

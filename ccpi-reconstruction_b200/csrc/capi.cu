@@ -727,6 +727,15 @@ int ccpi_plan_create(const ccpi_geometry *geometry, ccpi_plan **plan) {
 
 void ccpi_plan_destroy(ccpi_plan *plan) { delete plan; }
 
+int ccpi_plan_autotune(ccpi_plan *plan, void *stream, int chosen[2]) {
+  ccpi::g_last_error.clear();
+  if (!plan) {
+    set_error("ccpi_plan_autotune: null plan");
+    return 1;
+  }
+  return ccpi::plan_autotune(plan, cudaStream_t(stream), chosen);
+}
+
 long long ccpi_plan_voxels(const ccpi_plan *plan) { return plan ? plan->nvox : 0; }
 long long ccpi_plan_pixels(const ccpi_plan *plan) { return plan ? plan->npix : 0; }
 

@@ -919,7 +919,8 @@ void launch_cb_fp(const Geom &g, const float *vol, float *pix, const Epi &e, con
                   int grid, cudaStream_t st) {
   const size_t smem = cb_fp_smem(g);
   const int cap = g.nx + g.ny + 2;
-  const int r = cb_fp_rpl(g.nv);
+  const int r = (g.tune_rpl == 4 || g.tune_rpl == 8 || g.tune_rpl == 12) ? g.tune_rpl
+                                                                          : cb_fp_rpl(g.nv);
   const bool full = g.nv % (32 * r) == 0;
 #define CB_FP_GO(R, F)                                                                     \
   cb_fp_kernel<EPI, R, F><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap)

@@ -50,6 +50,9 @@ struct Geom {
   const float *vz;        // nz + 1: slice planes relative to src_z
   float inv_dz, pzbz, pzbz1, pzdv, z1, znm, pzdeps;
   int mid;                // first row above the source
+  // ---- launch shapes chosen by ccpi_plan_autotune (0: the built-in choice)
+  int tune_vw;            // parallel back projector: slices per lane (4, 8, 16)
+  int tune_rpl;           // cone forward projector: rows per lane (4, 8, 12)
 };
 
 // Epilogue operands shared by the fused projector epilogues.

@@ -757,4 +757,94 @@ int solve_batched(int n, const ccpi_plan *const *plans, int alg, const float *co
   return rc;
 }
 
+// Time the launch-shape candidates of this plan's projectors on scratch data
+// and keep the fastest (CUDA events on st; a warm-up launch, then the mean of
+// two).  Every candidate forms each ray's and each voxel's sum in the same
+// order, so projections do not depend on the choice; only the number of
+// per-CTA partial sums of squares (and so the FP64 summation order of the
+// CGLS step scalars) follows the forward projector's grid.
+int plan_autotune(ccpi_plan *p, cudaStream_t st, int *chosen) {
+  float *vol = nullptr, *pix = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = 0;
+  if (!cuda_ok(cudaMalloc(&vol, size_t(p->nvox) * 4), "autotune: volume") ||
+      !cuda_ok(cudaMalloc(&pix, size_t(p->npix) * 4), "autotune: sinogram") ||
+      !cuda_ok(cudaEventCreate(&e0), "autotune: event") ||
+      !cuda_ok(cudaEventCreate(&e1), "autotune: event"))
+    rc = 2;
+  if (rc == 0) {
+    k_fill(vol, p->nvox, 1.0f, st);
+    k_fill(pix, p->npix, 1.0f, st);
+  }
+  auto timed = [&](auto &&launch) -> float {
+    launch();
+    cudaEventRecord(e0, st);
+    launch();
+    launch();
+    cudaEventRecord(e1, st);
+    float ms = 0.0f;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+      return 1e30f;
+    return ms / 2.0f;
+  };
+  const Epi none{};
+  int best_fp = 0, best_bp = 0;
+  if (rc == 0 && p->g.kind == CCPI_PARALLEL) {
+    float t_best = 1e30f;
+    const int defgrid = p->fp_grid;
+    for (int per_sm : {3, 4, 5}) {
+      // defgrid is min(work tiles, 5 CTAs per SM)
+      const int gcand = std::max(1, std::min(defgrid, 148 * per_sm));
+      p->fp_grid = gcand;
+      const float t = timed([&] { pb_forward(p->g, vol, pix, EPI_STORE, none, p->fp_grid, p->err, st); });
+      if (t < t_best) {
+        t_best = t;
+        best_fp = gcand;
+      }
+    }
+    p->fp_grid = best_fp;
+    t_best = 1e30f;
+    for (int vw : {16, 8, 4}) {
+      if (p->g.map_type != 1 || p->g.nv != p->g.nz || p->g.nz % vw != 0)
+        continue;
+      p->g.tune_vw = vw;
+      const float t = timed([&] { pb_backward(p->g, pix, vol, EPI_STORE, none, p->err, st); });
+      if (t < t_best) {
+        t_best = t;
+        best_bp = vw;
+      }
+    }
+    p->g.tune_vw = best_bp;
+    p->bp_parts = pb_bp_tiles(p->g);
+  } else if (rc == 0) {
+    float t_best = 1e30f;
+    for (int rpl : {4, 8, 12}) {
+      p->g.tune_rpl = rpl;
+      const float t = timed([&] {
+        cb_forward(p->g, vol, pix, EPI_STORE, none, p->hrange, p->fp_grid, st);
+      });
+      if (t < t_best) {
+        t_best = t;
+        best_fp = rpl;
+      }
+    }
+    p->g.tune_rpl = best_fp;
+  }
+  if (rc == 0 && !cuda_ok(cudaStreamSynchronize(st), "autotune"))
+    rc = 2;
+  if (rc == 0 && !check_err(p))
+    rc = 16;
+  if (chosen) {
+    chosen[0] = p->g.kind == CCPI_PARALLEL ? p->fp_grid : p->g.tune_rpl;
+    chosen[1] = p->g.kind == CCPI_PARALLEL ? p->g.tune_vw : 0;
+  }
+  if (e0)
+    cudaEventDestroy(e0);
+  if (e1)
+    cudaEventDestroy(e1);
+  cudaFree(vol);
+  cudaFree(pix);
+  return rc;
+}
+
 } // namespace ccpi

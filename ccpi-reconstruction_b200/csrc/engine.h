@@ -30,6 +30,10 @@ int forward(const ccpi_plan *p, const float *vol, float *pix, int mode, const Ep
             cudaStream_t st);
 int backward(const ccpi_plan *p, const float *pix, float *vol, int mode, const Epi &e,
              cudaStream_t st);
+// Pick the fastest launch shapes for this plan on scratch data; chosen (may
+// be NULL) receives {forward grid or cone rows per lane, back projector
+// slices per lane or 0}.
+int plan_autotune(ccpi_plan *p, cudaStream_t st, int *chosen);
 size_t solve_workspace_bytes(const ccpi_plan *p, int alg, int niter);
 int solve(const ccpi_plan *p, int alg, const float *sino, float *x, int niter, double lambda,
           double *h_norms, int flags, void *ws, size_t ws_bytes, cudaStream_t st);

@@ -1002,7 +1002,9 @@ BpShape bp_shape(const Geom &g) {
   BpShape b;
   b.vw = 1;
   if (g.map_type == 1 && g.nv == g.nz) {
-    if (PB_BP_VW32 && g.nz % 32 == 0)
+    if ((g.tune_vw == 4 || g.tune_vw == 8 || g.tune_vw == 16) && g.nz % g.tune_vw == 0)
+      b.vw = g.tune_vw;
+    else if (PB_BP_VW32 && g.nz % 32 == 0)
       b.vw = 32;
     else if (PB_BP_VW16 && g.nz % 16 == 0)
       b.vw = 16;

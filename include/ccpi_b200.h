@@ -204,6 +204,16 @@ int ccpi_cb_create_sinogram(const ccpi_geometry *geometry,
  * The geometry's arrays are copied; the caller may free them. */
 int ccpi_plan_create(const ccpi_geometry *geometry, ccpi_plan **plan);
 void ccpi_plan_destroy(ccpi_plan *plan);
+/* Time this plan's projector launch shapes on scratch data and keep the
+ * fastest: the forward projector's grid (parallel beam) or rows per lane
+ * (cone beam), and the parallel back projector's slices per lane.  No
+ * counterpart in the reference (its block sizes are fixed).  Projections do
+ * not depend on the choice; CGLS step scalars may change in the last FP64
+ * bits (the number of partial sums follows the grid).  Call it after
+ * ccpi_plan_create and before any solve or session on the plan.  chosen
+ * (may be NULL) receives {grid or rows per lane, slices per lane or 0}.
+ * Allocates and frees scratch of one volume and one sinogram. */
+int ccpi_plan_autotune(ccpi_plan *plan, void *stream, int chosen[2]);
 /* Sizes of a plan's volume and sinogram in elements. */
 long long ccpi_plan_voxels(const ccpi_plan *plan);
 long long ccpi_plan_pixels(const ccpi_plan *plan);

@@ -232,3 +232,31 @@ def test_cgls_more_rows_than_one_projector_pass(cuda):
     g = O.parallel_geometry(shape, na, nh)
     r64 = O.solve(g, 0, sino.cpu().numpy().astype(np.float64), 3, fp64=True)
     assert rel_l2(x.cpu().numpy(), r64) <= 1e-4
+
+
+@pytest.mark.parametrize("kind", ["parallel", "cone"])
+def test_autotuned_plan_gives_the_same_results(kind, cuda):
+    """ccpi_plan_autotune changes launch shapes only: projections and SIRT
+    are bit-identical to the untuned plan, CGLS agrees to FP64 rounding of
+    its step scalars."""
+    import torch
+    from ccpi.reconstruction.device import cone_plan, parallel_plan
+    mk = (lambda: parallel_plan((48, 48, 32), 60, 72)) if kind == "parallel" else \
+        (lambda: cone_plan(24, 1.0, 30, 32, 1.0, 60.0, 60.0))
+    a, b = mk(), mk()
+    chosen = b.autotune()
+    assert chosen[0] > 0
+    rng = np.random.default_rng(17)
+    x = torch.from_numpy(rng.random(a.shape).astype(np.float32)).to(cuda)
+    sa, sb = a.forward(x), b.forward(x)
+    assert torch.equal(sa, sb)
+    assert torch.equal(a.backward(sa), b.backward(sb))
+    for alg, exact in ((1, True), (0, False)):
+        xa = torch.zeros(a.shape, device=cuda)
+        xb = torch.zeros(b.shape, device=cuda)
+        a.solve(alg, sa, xa, 5)
+        b.solve(alg, sb, xb, 5)
+        if exact:
+            assert torch.equal(xa, xb)
+        else:
+            assert rel_l2(xb.cpu().numpy(), xa.cpu().numpy()) <= 1e-6
