@@ -559,13 +559,15 @@ __global__ void __launch_bounds__(kBpThreads)
 // column; rows ascending, each row feeding its slice k and the neighbour
 // k -/+ 1), then the edge rows of every ray (below the band descending,
 // above it ascending).  Here one CTA owns one column and each thread owns
-// NZT of its voxels.  Rays are staged per angle chunk; for a stage of
-// kGaStage rays the threads first compute, per detector row, the slice
-// index and the d_conv-scaled pixel value and record for every slice K the
-// first band row whose index reaches K (k is monotone in the row).  Each
-// voxel thread then walks exactly the rows that touch its voxel, in the
-// reference's order, so every voxel's sum is formed in the same order with
-// the same unfused float operations as the reference.
+// NZT of its voxels.  Rays are staged per angle chunk.  For a stage of
+// kGaStage rays each thread loads its band rows (RMAX per ray, all loads in
+// flight together), forms every row's two contributions exactly as the
+// reference does (p (mz - a0) for the row's slice k, p (a1 - mz) for its
+// neighbour) and records, for every slice K, the first band row whose index
+// reaches K (k is monotone in the row).  Each voxel thread then adds, per
+// ray, exactly the contributions that go to its voxel, in the reference's
+// order, so every voxel's sum is formed in the same order with the same
+// unfused float operations as the reference.
 constexpr int kGaThreads = 256;
 constexpr int kGaChunk = 64;
 constexpr int kGaRays = kBpMaxRaysPerAngle; // slots per angle
@@ -575,20 +577,6 @@ constexpr int kGaRays = kBpMaxRaysPerAngle; // slots per angle
 constexpr int kGaStage = CB_GA_STAGE;
 
 __host__ __device__ inline int round4(int n) { return (n + 3) & ~3; }
-
-// Asynchronous global -> shared copies (cp.async), so that every row of a
-// stage is in flight at once instead of one round trip per ray.
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-}
 
 // Shared-memory layout of cb_bp_gather (offsets in 4-byte words).
 struct GaLayout {
@@ -650,8 +638,10 @@ __device__ int cb_ga_stage_rays(const Geom &g, int ac, int nac, double x0, doubl
   return off[nac];
 }
 
-template <int EPI, int NZT>
-__global__ void __launch_bounds__(kGaThreads)
+// Register bound: 4 CTAs per SM for one voxel per thread; taller columns
+// need more shared memory per CTA, which allows 3 (or 2) anyway.
+template <int EPI, int NZT, int RMAX>
+__global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
     cb_bp_gather(Geom g, const float *__restrict__ pix, float *__restrict__ vol, Epi e,
                  int *err) {
   extern __shared__ unsigned char smem_raw[];
@@ -669,9 +659,6 @@ __global__ void __launch_bounds__(kGaThreads)
   float *drow = reinterpret_cast<float *>(W + L.drow); // their d_conv rows
   const int frs = round4(nz + 2), prs = round4(nv);
   __shared__ int s_minv, s_maxv, s_ovf;
-  // slice index of the first and last band row of each staged ray; the
-  // first-row table fr[K] is only written for kfirst < K <= klast
-  __shared__ int kfirst[kGaStage], klast[kGaStage];
   const int tid = threadIdx.x;
   const int col = blockIdx.x;
   const int i = col / g.ny, j = col - (col / g.ny) * g.ny;
@@ -704,19 +691,13 @@ __global__ void __launch_bounds__(kGaThreads)
   __syncthreads();
   const int min_v = s_minv, max_v = s_maxv;
   const int nb = max_v - min_v;
-  // 16-byte copies need 16-byte aligned rows (nv a multiple of 4)
-  const bool vec16 = (nv & 3) == 0;
   const int lo_end = min(mid, max_v);         // lower band rows [min_v, lo_end)
   const int up_begin = max(mid, min_v);       // upper band rows [up_begin, max_v)
   const float pzbz = g.pzbz, pzbz1 = g.pzbz1, inv_dz = g.inv_dz;
-  float acc[NZT], vzk[NZT], vzk1[NZT];
+  float acc[NZT];
 #pragma unroll
-  for (int q = 0; q < NZT; q++) {
-    const int K = min(tid + q * kGaThreads, nzm1);
+  for (int q = 0; q < NZT; q++)
     acc[q] = 0.0f;
-    vzk[q] = svz[K];
-    vzk1[q] = svz[K + 1];
-  }
 
   // ---- band rows of every ray (c2D.cpp:680-713)
   for (int ac = 0; nb > 0 && ac < g.na; ac += kGaChunk) {
@@ -725,81 +706,84 @@ __global__ void __launch_bounds__(kGaThreads)
                                       off, map, &s_ovf);
     for (int s0 = 0; s0 < nseg; s0 += kGaStage) {
       const int ns = min(kGaStage, nseg - s0);
-      // start the copies of the stage's pixel and d_conv rows (band only)
-      for (int s = 0; s < ns; s++) {
-        const int m = map[s0 + s];
+      // 1) this thread's band rows v = min_v + tid + r * 256 of every staged
+      //    ray: pixel and d_conv values, all loads issued together
+      float pv[kGaStage][RMAX], dv[kGaStage][RMAX];
+#pragma unroll
+      for (int s = 0; s < kGaStage; s++) {
+        const int m = map[s0 + (s < ns ? s : 0)];
         const int a = ac + m / kGaRays, h = seg_h[m];
         const float *prw = pix + (i64(a) * g.nh + h) * nv;
         const float *drw = g.dconv + i64(h) * nv;
-        float *pr = prow + s * prs, *dr = drow + s * prs;
-        if (vec16) {
-          for (int v = (min_v & ~3) + 4 * tid; v < max_v; v += 4 * blockDim.x) {
-            cp_async16(pr + v, prw + v);
-            cp_async16(dr + v, drw + v);
-          }
-        } else {
-          for (int v = min_v + tid; v < max_v; v += blockDim.x) {
-            cp_async4(pr + v, prw + v);
-            cp_async4(dr + v, drw + v);
-          }
+#pragma unroll
+        for (int r = 0; r < RMAX; r++) {
+          const int v = min_v + tid + r * kGaThreads;
+          const bool ok = s < ns && v < max_v;
+          pv[s][r] = ok ? __ldg(prw + v) : 0.0f;
+          dv[s][r] = ok ? __ldg(drw + v) : 0.0f;
         }
       }
-      // meanwhile: first band row of every slice index, per ray
-      for (int s = 0; s < ns; s++) {
-        const float av = __fmul_rn(seg_a0[map[s0 + s]], inv_dz);
-        int *f = fr + s * frs;
-        for (int v = min_v + tid; v < max_v; v += blockDim.x) {
-          const int k = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[v])));
-          if (v == min_v)
-            kfirst[s] = k;
-          else {
-            const int kp = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[v - 1])));
-            for (int K = max(kp + 1, 0); K <= min(k, nz + 1); K++)
-              f[K] = v;
-          }
-          if (v == max_v - 1)
-            klast[s] = k;
-        }
-      }
-      cp_async_wait_all();
-      __syncthreads();
-      for (int s = 0; s < ns; s++) {
+      // 2) per ray: the first band row of every slice index (the whole
+      //    table: below the first row's slice min_v, above the last row's
+      //    max_v) and each row's two contributions as the reference forms
+      //    them (c2D.cpp:694-711): c1 = p (mz - a0) goes to slice k, c2 =
+      //    p (a1 - mz) to k - 1 below the source row, to k + 1 from it on
+#pragma unroll
+      for (int s = 0; s < kGaStage; s++) {
+        if (s >= ns)
+          break;
         const int m = map[s0 + s];
         const float a0 = seg_a0[m], a1 = seg_a1[m];
+        const float av = __fmul_rn(a0, inv_dz);
+        int *f = fr + s * frs;
+        const int kf = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[min_v])));
+        const int kl = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[max_v - 1])));
+        for (int K = tid; K <= nz + 1; K += kGaThreads) {
+          if (K <= kf)
+            f[K] = min_v;
+          else if (K > kl)
+            f[K] = max_v;
+        }
+        float *c1 = prow + s * prs, *c2 = drow + s * prs;
+#pragma unroll
+        for (int r = 0; r < RMAX; r++) {
+          const int v = min_v + tid + r * kGaThreads;
+          if (v < max_v) {
+            const int k = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[v])));
+            if (v > min_v) {
+              const int kp = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[v - 1])));
+              for (int K = max(kp + 1, 0); K <= min(k, nz + 1); K++)
+                f[K] = v;
+            }
+            const int kz = min(max(v < mid ? k : k + 1, 0), nz);
+            const float mz = fmin_ref(__fmul_rn(svz[kz], siz[v]), a1);
+            const float p = __fmul_rn(pv[s][r], dv[s][r]);
+            c1[v] = __fmul_rn(p, __fsub_rn(mz, a0));
+            c2[v] = __fmul_rn(p, __fsub_rn(a1, mz));
+          }
+        }
+      }
+      __syncthreads();
+      // 3) each voxel adds its rows' contributions in the reference's order
+      for (int s = 0; s < ns; s++) {
         const int *f = fr + s * frs;
-        const float *pr = prow + s * prs, *dr = drow + s * prs;
-        const int kf = kfirst[s], kl = klast[s];
-        // first band row whose slice index reaches K
-        auto first = [&](int K) { return K <= kf ? min_v : (K > kl ? max_v : f[max(K, 0)]); };
+        const float *c1 = prow + s * prs, *c2 = drow + s * prs;
 #pragma unroll
         for (int q = 0; q < NZT; q++) {
           const int K = tid + q * kGaThreads;
           if (K >= nz)
             continue;
-          // lower band: rows with k in {K, K+1}; k == K feeds K, k == K+1
-          // feeds its neighbour k - 1 == K
-          const int fk = first(K), fk1 = first(K + 1);
-          for (int v = fk, ve = min(first(K + 2), lo_end); v < ve; v++) {
-            const float p = __fmul_rn(pr[v], dr[v]);
-            if (v < fk1) {
-              const float mz = fmin_ref(__fmul_rn(vzk[q], siz[v]), a1);
-              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(mz, a0)));
-            } else {
-              const float mz = fmin_ref(__fmul_rn(vzk1[q], siz[v]), a1);
-              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(a1, mz)));
-            }
-          }
-          // upper band: rows with k in {K-1, K}; k == K-1 feeds k + 1 == K
-          for (int v = max(first(K - 1), up_begin), ve = min(fk1, max_v); v < ve; v++) {
-            const float p = __fmul_rn(pr[v], dr[v]);
-            if (v < fk) {
-              const float mz = fmin_ref(__fmul_rn(vzk[q], siz[v]), a1);
-              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(a1, mz)));
-            } else {
-              const float mz = fmin_ref(__fmul_rn(vzk1[q], siz[v]), a1);
-              acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(mz, a0)));
-            }
-          }
+          const int fm = K >= 1 ? f[K - 1] : min_v, f0 = f[K], f1 = f[K + 1];
+          float t = acc[q];
+          // below the source row: rows of slice K give c1, then rows of
+          // slice K + 1 give c2 (their neighbour k - 1 == K)
+          for (int v = f0, ve = min(f[K + 2], lo_end); v < ve; v++)
+            t = __fadd_rn(t, (v < f1 ? c1 : c2)[v]);
+          // from the source row on: rows of slice K - 1 give c2 (their
+          // neighbour k + 1 == K), then rows of slice K give c1
+          for (int v = max(fm, up_begin), ve = min(f1, max_v); v < ve; v++)
+            t = __fadd_rn(t, (v < f0 ? c2 : c1)[v]);
+          acc[q] = t;
         }
       }
       __syncthreads();
@@ -942,10 +926,12 @@ size_t cb_bp_atomic_smem(const Geom &g) {
 size_t cb_bp_gather_smem(const Geom &g) { return size_t(GaLayout(g.nz, g.nv).total) * 4; }
 // voxels per thread of the deterministic gather, 0 if it does not apply
 int cb_bp_gather_nzt(const Geom &g) {
-  if (cb_bp_gather_smem(g) > 200 * 1024)
+  if (cb_bp_gather_smem(g) > 200 * 1024 || g.nv > 4 * kGaThreads)
     return 0;
   return g.nz <= kGaThreads ? 1 : g.nz <= 2 * kGaThreads ? 2 : g.nz <= 4 * kGaThreads ? 4 : 0;
 }
+// band rows per thread of the deterministic gather (nv <= 1024)
+int cb_bp_gather_rmax(const Geom &g) { return (g.nv + kGaThreads - 1) / kGaThreads; }
 } // namespace
 
 size_t cb_bp_smem(const Geom &g) {
@@ -971,10 +957,12 @@ int cb_prepare(const Geom &g) {
     if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bp) != cudaSuccess)
       e2 = cudaErrorInvalidValue;
   if (cb_bp_gather_nzt(g)) {
-#define CB_GA_ALL(Z)                                                                       \
-  (const void *)cb_bp_gather<EPI_STORE, Z>, (const void *)cb_bp_gather<EPI_NORM, Z>,        \
-      (const void *)cb_bp_gather<EPI_SIRT, Z>, (const void *)cb_bp_gather<EPI_MLEM, Z>
+#define CB_GA_EPI(Z, R)                                                                    \
+  (const void *)cb_bp_gather<EPI_STORE, Z, R>, (const void *)cb_bp_gather<EPI_NORM, Z, R>,  \
+      (const void *)cb_bp_gather<EPI_SIRT, Z, R>, (const void *)cb_bp_gather<EPI_MLEM, Z, R>
+#define CB_GA_ALL(Z) CB_GA_EPI(Z, 1), CB_GA_EPI(Z, 2), CB_GA_EPI(Z, 3), CB_GA_EPI(Z, 4)
     const void *gas[] = {CB_GA_ALL(1), CB_GA_ALL(2), CB_GA_ALL(4)};
+#undef CB_GA_EPI
 #undef CB_GA_ALL
     for (const void *f : gas)
       if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ga) != cudaSuccess)
@@ -1009,19 +997,27 @@ template <int EPI>
 void launch_cb_bp(const Geom &g, const float *pix, float *vol, const Epi &e, int *err,
                   cudaStream_t st) {
   const int ncol = g.nx * g.ny;
+  const size_t gsm = cb_bp_gather_smem(g);
+  const int rmax = cb_bp_gather_rmax(g);
+#define CB_GA_GO(Z)                                                                        \
+  (rmax == 1   ? cb_bp_gather<EPI, Z, 1><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err)  \
+   : rmax == 2 ? cb_bp_gather<EPI, Z, 2><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err)  \
+   : rmax == 3 ? cb_bp_gather<EPI, Z, 3><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err)  \
+               : cb_bp_gather<EPI, Z, 4><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err))
   switch (cb_bp_gather_nzt(g)) {
   case 1:
-    cb_bp_gather<EPI, 1><<<ncol, kGaThreads, cb_bp_gather_smem(g), st>>>(g, pix, vol, e, err);
+    CB_GA_GO(1);
     break;
   case 2:
-    cb_bp_gather<EPI, 2><<<ncol, kGaThreads, cb_bp_gather_smem(g), st>>>(g, pix, vol, e, err);
+    CB_GA_GO(2);
     break;
   case 4:
-    cb_bp_gather<EPI, 4><<<ncol, kGaThreads, cb_bp_gather_smem(g), st>>>(g, pix, vol, e, err);
+    CB_GA_GO(4);
     break;
   default:
     cb_bp_kernel<EPI><<<ncol, kBpThreads, cb_bp_atomic_smem(g), st>>>(g, pix, vol, e, err);
   }
+#undef CB_GA_GO
 }
 } // namespace
 
