@@ -572,7 +572,7 @@ constexpr int kGaThreads = 256;
 constexpr int kGaChunk = 64;
 constexpr int kGaRays = kBpMaxRaysPerAngle; // slots per angle
 #ifndef CB_GA_STAGE
-#define CB_GA_STAGE 4
+#define CB_GA_STAGE 3
 #endif
 constexpr int kGaStage = CB_GA_STAGE;
 
