@@ -574,6 +574,9 @@ constexpr int kGaRays = kBpMaxRaysPerAngle; // slots per angle
 #ifndef CB_GA_STAGE
 #define CB_GA_STAGE 3
 #endif
+#ifndef CB_GA_FAST
+#define CB_GA_FAST 1
+#endif
 constexpr int kGaStage = CB_GA_STAGE;
 
 __host__ __device__ inline int round4(int n) { return (n + 3) & ~3; }
@@ -659,13 +662,13 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
   float *drow = reinterpret_cast<float *>(W + L.drow); // their d_conv rows
   const int frs = round4(nz + 2), prs = round4(nv);
   __shared__ int s_minv, s_maxv, s_ovf;
+  __shared__ int s_kf[kGaStage], s_kl[kGaStage]; // slices of a staged ray's first/last band row
+  // the column's square; kept in shared memory so that its FP64 corners
+  // hold no registers through the row and voxel phases
+  __shared__ double s_box[4];
   const int tid = threadIdx.x;
   const int col = blockIdx.x;
   const int i = col / g.ny, j = col - (col / g.ny) * g.ny;
-  const double x0 = g.origin[0] + double(i) * g.size[0];
-  const double xn = g.origin[0] + double(i + 1) * g.size[0];
-  const double y0 = g.origin[1] + double(j) * g.size[1];
-  const double yn = g.origin[1] + double(j + 1) * g.size[1];
   for (int t = tid; t <= nz; t += blockDim.x)
     svz[t] = g.vz[t];
   for (int t = tid; t < nv; t += blockDim.x) {
@@ -676,12 +679,16 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
     s_minv = 0;
     s_maxv = nv;
     s_ovf = 0;
+    s_box[0] = g.origin[0] + double(i) * g.size[0];
+    s_box[1] = g.origin[0] + double(i + 1) * g.size[0];
+    s_box[2] = g.origin[1] + double(j) * g.size[1];
+    s_box[3] = g.origin[1] + double(j + 1) * g.size[1];
   }
   __syncthreads();
   // band limits over every ray of the column (c2D.cpp:657-676)
   for (int a = tid; a < g.na; a += blockDim.x) {
     int lo = 0, hi = nv;
-    cb_column_rays(g, a, x0, xn, y0, yn, [&](int, float a0, float) {
+    cb_column_rays(g, a, s_box[0], s_box[1], s_box[2], s_box[3], [&](int, float a0, float) {
       lo = max(lo, int(ceilf(__fadd_rn(g.pzdeps, __fdiv_rn(g.z1, a0)))));
       hi = min(hi, int(floorf(__fadd_rn(g.pzdv, __fdiv_rn(g.znm, a0)))));
     });
@@ -698,12 +705,25 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
 #pragma unroll
   for (int q = 0; q < NZT; q++)
     acc[q] = 0.0f;
+  // this thread's band rows v = min_v + tid + r * 256 are the same for every
+  // ray: their z tables stay in registers (sd: delta_z of v, sp: of v - 1,
+  // si: inv_delz of v)
+  float rsd[RMAX], rsp[RMAX], rsi[RMAX];
+#pragma unroll
+  for (int r = 0; r < RMAX; r++) {
+    const int v = min_v + tid + r * kGaThreads;
+    const bool in = v < max_v;
+    rsd[r] = in ? sdz[v] : 0.0f;
+    rsp[r] = (in && v > min_v) ? sdz[v - 1] : 0.0f;
+    rsi[r] = in ? siz[v] : 0.0f;
+  }
+  const float sd_first = nb > 0 ? sdz[min_v] : 0.0f, sd_last = nb > 0 ? sdz[max_v - 1] : 0.0f;
 
   // ---- band rows of every ray (c2D.cpp:680-713)
   for (int ac = 0; nb > 0 && ac < g.na; ac += kGaChunk) {
     const int nac = min(kGaChunk, g.na - ac);
-    const int nseg = cb_ga_stage_rays(g, ac, nac, x0, xn, y0, yn, seg_h, seg_a0, seg_a1, cnt,
-                                      off, map, &s_ovf);
+    const int nseg = cb_ga_stage_rays(g, ac, nac, s_box[0], s_box[1], s_box[2], s_box[3], seg_h,
+                                      seg_a0, seg_a1, cnt, off, map, &s_ovf);
     for (int s0 = 0; s0 < nseg; s0 += kGaStage) {
       const int ns = min(kGaStage, nseg - s0);
       // 1) this thread's band rows v = min_v + tid + r * 256 of every staged
@@ -736,27 +756,47 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
         const float a0 = seg_a0[m], a1 = seg_a1[m];
         const float av = __fmul_rn(a0, inv_dz);
         int *f = fr + s * frs;
-        const int kf = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[min_v])));
-        const int kl = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[max_v - 1])));
+        const int kf = int(__fadd_rn(pzbz, __fmul_rn(av, sd_first)));
+        const int kl = int(__fadd_rn(pzbz, __fmul_rn(av, sd_last)));
+#if CB_GA_FAST
+        // only voxels kf - 1 .. kl + 1 receive rows of this ray, and they
+        // read entries kf - 2 .. kl + 3: the band rows' transitions write
+        // (kf, kl], six threads write the ends
+        if (tid < 6) {
+          const int K = tid < 3 ? kf - tid : kl + tid - 2;
+          if (K >= 0 && K <= nz + 1)
+            f[K] = tid < 3 ? min_v : max_v;
+        }
+        if (tid == 0) {
+          s_kf[s] = kf;
+          s_kl[s] = kl;
+        }
+#else
         for (int K = tid; K <= nz + 1; K += kGaThreads) {
           if (K <= kf)
             f[K] = min_v;
           else if (K > kl)
             f[K] = max_v;
         }
+#endif
         float *c1 = prow + s * prs, *c2 = drow + s * prs;
 #pragma unroll
         for (int r = 0; r < RMAX; r++) {
           const int v = min_v + tid + r * kGaThreads;
           if (v < max_v) {
-            const int k = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[v])));
+            const int k = int(__fadd_rn(pzbz, __fmul_rn(av, rsd[r])));
             if (v > min_v) {
-              const int kp = int(__fadd_rn(pzbz, __fmul_rn(av, sdz[v - 1])));
-              for (int K = max(kp + 1, 0); K <= min(k, nz + 1); K++)
-                f[K] = v;
+              const int kp = int(__fadd_rn(pzbz, __fmul_rn(av, rsp[r])));
+#if CB_GA_FAST
+              if (k == kp + 1 && k >= 0 && k <= nz + 1)
+                f[k] = v; // the usual step: one slice per row change
+              else
+#endif
+                for (int K = max(kp + 1, 0); K <= min(k, nz + 1); K++)
+                  f[K] = v;
             }
             const int kz = min(max(v < mid ? k : k + 1, 0), nz);
-            const float mz = fmin_ref(__fmul_rn(svz[kz], siz[v]), a1);
+            const float mz = fmin_ref(__fmul_rn(svz[kz], rsi[r]), a1);
             const float p = __fmul_rn(pv[s][r], dv[s][r]);
             c1[v] = __fmul_rn(p, __fsub_rn(mz, a0));
             c2[v] = __fmul_rn(p, __fsub_rn(a1, mz));
@@ -768,11 +808,18 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
       for (int s = 0; s < ns; s++) {
         const int *f = fr + s * frs;
         const float *c1 = prow + s * prs, *c2 = drow + s * prs;
+#if CB_GA_FAST
+        const int klo = s_kf[s] - 1, khi = s_kl[s] + 1;
+#endif
 #pragma unroll
         for (int q = 0; q < NZT; q++) {
           const int K = tid + q * kGaThreads;
           if (K >= nz)
             continue;
+#if CB_GA_FAST
+          if (K < klo || K > khi)
+            continue; // no row of this ray feeds voxel K
+#endif
           const int fm = K >= 1 ? f[K - 1] : min_v, f0 = f[K], f1 = f[K + 1];
           float t = acc[q];
           // below the source row: rows of slice K give c1, then rows of
@@ -794,8 +841,8 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
   if (min_v > 0 || max_v < nv) {
     for (int ac = 0; ac < g.na; ac += kGaChunk) {
       const int nac = min(kGaChunk, g.na - ac);
-      const int nseg = cb_ga_stage_rays(g, ac, nac, x0, xn, y0, yn, seg_h, seg_a0, seg_a1, cnt,
-                                        off, map, &s_ovf);
+      const int nseg = cb_ga_stage_rays(g, ac, nac, s_box[0], s_box[1], s_box[2], s_box[3],
+                                        seg_h, seg_a0, seg_a1, cnt, off, map, &s_ovf);
       for (int s = 0; s < nseg; s++) {
         const int m = map[s];
         const int a = ac + m / kGaRays, h = seg_h[m];
