@@ -55,6 +55,11 @@ def _load():
                                                ctypes.c_float, _c_int, _f32p]
     lib.ccpi_ring_filter_aml.argtypes = [_vp, _c_int, _c_int, _c_int, _c_dbl, _c_dbl, _c_int,
                                          _vp]
+    lib.ccpi_pb_high_peaks.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_dbl, _c_int, _c_int,
+                                       _f32p]
+    lib.ccpi_pb_column_ring_artefacts.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_int, _f32p]
+    lib.ccpi_high_peaks.argtypes = [_vp, _c_int, _c_int, _c_int, _c_dbl, _c_int, _vp]
+    lib.ccpi_ring_filter_column.argtypes = [_vp, _c_int, _c_int, _c_int, _vp]
     lib.ccpi_pb_forward_project.argtypes = [_f32p, _c_int, _c_int, _c_int, _f32p, _c_int,
                                             _c_int, _vp, _i32p]
     lib.ccpi_pb_backward_project.argtypes = [_f32p, _c_int, _c_int, _c_int, _f32p, _c_dbl,

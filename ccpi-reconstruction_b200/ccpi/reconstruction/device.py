@@ -250,3 +250,30 @@ def ring_filter_aml(sino, param_n, param_r, num_series):
                                            torch.cuda.current_stream(sino.device).cuda_stream)),
             "ccpi_ring_filter_aml")
     return sino
+
+
+def _log_sinogram(sino):
+    if not (sino.is_cuda and sino.dtype == torch.float32 and sino.is_contiguous()
+            and sino.dim() == 3):
+        raise ValueError("sinogram must be a contiguous 3-D float32 CUDA tensor")
+    return sino.shape, ctypes.c_void_p(torch.cuda.current_stream(sino.device).cuda_stream)
+
+
+def high_peaks(sino, jump, num_pix):
+    """High-peaks filter (``ccpi_high_peaks``) on a log sinogram in the
+    internal layout (n_angles, n_h, n_v), in place, on torch's current
+    stream; returns sino."""
+    (na, nh, nv), st = _log_sinogram(sino)
+    N.check(N.lib.ccpi_high_peaks(ctypes.c_void_p(sino.data_ptr()), na, nh, nv, float(jump),
+                                  int(num_pix), st), "ccpi_high_peaks")
+    return sino
+
+
+def ring_filter_column(sino):
+    """Column ring-artefact filter (``ccpi_ring_filter_column``) on a log
+    sinogram in the internal layout (n_angles, n_h, n_v), in place, on
+    torch's current stream; returns sino."""
+    (na, nh, nv), st = _log_sinogram(sino)
+    N.check(N.lib.ccpi_ring_filter_column(ctypes.c_void_p(sino.data_ptr()), na, nh, nv, st),
+            "ccpi_ring_filter_column")
+    return sino

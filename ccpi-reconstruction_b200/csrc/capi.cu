@@ -367,6 +367,51 @@ int solve_on_host_data(HostGeometry &G, int alg, const float *sino_host, bool ra
 
 } // namespace
 
+namespace {
+// A sinogram filter on host pixels (n_angles, n_v, n_h): -log unless the
+// data are already logs, the internal layout [a][h][v], the filter, back to
+// (n_angles, n_v, n_h) and, for transmission input, exp(-x) with the C
+// library's expf, as the reference's filter wrapper does
+// (diamond_wrapper.cpp:28-48).
+template <class F>
+int host_sino_filter(const char *name, const float *pixels, int na, int nv, int nh, int is_log,
+                     float *out, F &&filter) {
+  if (!pixels || !out || na < 1 || nv < 1 || nh < 1) {
+    set_error(std::string(name) + ": need pixels (n_angles, n_v, n_h >= 1) and an output buffer");
+    return 1;
+  }
+  const i64 n = i64(na) * nv * nh;
+  std::vector<float> logged(size_t(n), 0.0f);
+  if (is_log)
+    std::memcpy(logged.data(), pixels, size_t(n) * 4);
+  else
+    neglog_host(pixels, logged.data(), n);
+  DevBuf raw, sino;
+  if (!raw.alloc(n * 4) || !sino.alloc(n * 4))
+    return 2;
+  cudaStream_t st = 0;
+  if (!ccpi::cuda_ok(cudaMemcpy(raw.p, logged.data(), n * 4, cudaMemcpyHostToDevice),
+                     "upload pixels"))
+    return 2;
+  ccpi::k_pack_parallel(raw.f(), sino.f(), na, nv, nh, nv, 0, st); // -> [a][h][v]
+  const int rc = filter(sino.f(), st);
+  if (rc)
+    return rc;
+  ccpi::k_unpack_parallel(sino.f(), raw.f(), na, nh, nv, st); // -> [a][v][h]
+  if (!ccpi::cuda_ok(cudaMemcpy(logged.data(), raw.p, n * 4, cudaMemcpyDeviceToHost),
+                     "download pixels"))
+    return 2;
+  if (is_log) {
+    std::memcpy(out, logged.data(), size_t(n) * 4);
+  } else {
+#pragma omp parallel for schedule(static)
+    for (i64 i = 0; i < n; i++)
+      out[i] = std::exp(-logged[size_t(i)]);
+  }
+  return 0;
+}
+} // namespace
+
 extern "C" {
 
 const char *ccpi_last_error(void) { return ccpi::g_last_error.c_str(); }
@@ -547,6 +592,38 @@ int ccpi_ring_filter_aml(float *d_sino, int n_angles, int n_h, int n_v, double p
   ccpi::g_last_error.clear();
   return ccpi::aml_ring_filter(d_sino, n_angles, n_h, n_v, param_n, param_r, num_series,
                                cudaStream_t(stream));
+}
+
+int ccpi_pb_high_peaks(const float *pixels, int na, int nv, int nh, double jump, int num_pix,
+                       int is_pixels_in_log, float *out) {
+  ccpi::g_last_error.clear();
+  if (pixels && out && na >= 1 && ccpi::high_peaks_check(na, jump, num_pix))
+    return 1;
+  return host_sino_filter("ccpi_pb_high_peaks", pixels, na, nv, nh, is_pixels_in_log, out,
+                          [&](float *d, cudaStream_t st) {
+                            return ccpi::high_peaks_filter(d, na, nh, nv, jump, num_pix, st);
+                          });
+}
+
+int ccpi_pb_column_ring_artefacts(const float *pixels, int na, int nv, int nh,
+                                  int is_pixels_in_log, float *out) {
+  ccpi::g_last_error.clear();
+  return host_sino_filter("ccpi_pb_column_ring_artefacts", pixels, na, nv, nh, is_pixels_in_log,
+                          out, [&](float *d, cudaStream_t st) {
+                            return ccpi::column_ring_filter(d, na, nh, nv, st);
+                          });
+}
+
+int ccpi_high_peaks(float *d_sino, int n_angles, int n_h, int n_v, double jump, int num_pix,
+                    void *stream) {
+  ccpi::g_last_error.clear();
+  return ccpi::high_peaks_filter(d_sino, n_angles, n_h, n_v, jump, num_pix,
+                                 cudaStream_t(stream));
+}
+
+int ccpi_ring_filter_column(float *d_sino, int n_angles, int n_h, int n_v, void *stream) {
+  ccpi::g_last_error.clear();
+  return ccpi::column_ring_filter(d_sino, n_angles, n_h, n_v, cudaStream_t(stream));
 }
 
 int ccpi_pb_forward_project(const float *volume, int vx, int vy, int vz, const float *angles_deg,

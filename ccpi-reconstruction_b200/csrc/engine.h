@@ -48,5 +48,13 @@ int solve_batched(int n, const ccpi_plan *const *plans, int alg, const float *co
 // (aml.cu); synchronises st.
 int aml_ring_filter(float *d_sino, int na, int nh, int nv, double param_n, double param_r,
                     int num_series, cudaStream_t st);
+// High-peaks and column ring-artefact filters on a device sinogram
+// [angle][h][v], in place (prefilter.cu); launched on st, not waited for.
+int high_peaks_filter(float *d_sino, int na, int nh, int nv, double jump, int num_pix,
+                      cudaStream_t st);
+int column_ring_filter(float *d_sino, int na, int nh, int nv, cudaStream_t st);
+// The high-peaks parameter checks alone (no CUDA call); 1 and an error
+// message when jump < 0 or num_pix is outside [1, na).
+int high_peaks_check(int na, double jump, int num_pix);
 
 } // namespace ccpi

@@ -143,6 +143,32 @@ int ccpi_ring_filter_aml(float *d_sino, int n_angles, int n_h, int n_v,
                          double param_n, double param_r, int num_series,
                          void *stream);
 
+/* The high-peaks filter of the reference's Diamond pre-processing
+ * (CCPi::Diamond::high_peaks_before, Core/src/diamond.cpp:513-617; the
+ * reference runs it on the -log sinogram when its configuration asks,
+ * diamond.cpp:383-384, and has no Python call for it).  pixels and out:
+ * (n_angles, n_v, n_h); with is_pixels_in_log == 0 they are transmission
+ * (filtered as -log, returned as exp(-filtered)), else logs.  jump < 0 and
+ * num_pix outside [1, n_angles) are errors (the reference prints them and
+ * leaves the data unfiltered). */
+int ccpi_pb_high_peaks(const float *pixels, int n_angles, int n_v, int n_h,
+                       double jump, int num_pix, int is_pixels_in_log,
+                       float *out);
+
+/* The column ring-artefact filter (CCPi::remove_column_ring_artefacts,
+ * Core/src/diamond.cpp:619-658, reached through the reference's
+ * configuration, diamond.cpp:814-816): every detector element loses its
+ * mean over the angles.  Layout and is_pixels_in_log as ccpi_pb_high_peaks. */
+int ccpi_pb_column_ring_artefacts(const float *pixels, int n_angles, int n_v,
+                                  int n_h, int is_pixels_in_log, float *out);
+
+/* The two filters above on a device log sinogram in the internal layout
+ * (n_angles, n_h, n_v), in place, launched on `stream` (not waited for). */
+int ccpi_high_peaks(float *d_sino, int n_angles, int n_h, int n_v, double jump,
+                    int num_pix, void *stream);
+int ccpi_ring_filter_column(float *d_sino, int n_angles, int n_h, int n_v,
+                            void *stream);
+
 /* parallelbeam.alg.pb_forward_project (diamond_wrapper.cpp:421-556):
  * volume (vx, vy, vz) -> (n_angles, n_v_padded, max(vx, vy)).  With
  * out == NULL only out_dims is filled. */

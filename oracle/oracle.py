@@ -102,7 +102,11 @@ def restate():
             fn.restype = _c_int
             getattr(lib, f"rs_regularize_{suf}").argtypes = [_c_int, _c_int, _c_int, _c_int, p, p]
         lib.rs_neglog_f32.argtypes = [_f32p, _f32p, ctypes.c_longlong]
+        lib.rs_expneg_f32.argtypes = [_f32p, _f32p, ctypes.c_longlong]
         lib.rs_aml_ring_f32.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_dbl, _c_dbl, _c_int]
+        lib.rs_high_peaks_f32.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_dbl, _c_int]
+        lib.rs_high_peaks_f32.restype = _c_int
+        lib.rs_column_ring_f32.argtypes = [_f32p, _c_int, _c_int, _c_int]
         _rs = lib
     return _rs
 
@@ -148,6 +152,15 @@ def neglog(p):
     p = np.ascontiguousarray(p, np.float32)
     out = np.empty_like(p)
     restate().rs_neglog_f32(p, out, p.size)
+    return out
+
+
+def expneg(p):
+    """exp(-p) with the C library's expf (the reference wrapper's way back
+    from logs to transmission)."""
+    p = np.ascontiguousarray(p, np.float32)
+    out = np.empty_like(p)
+    restate().rs_expneg_f32(p, out, p.size)
     return out
 
 
@@ -266,6 +279,8 @@ def reference():
                                                                      _c_dbl, _f32p]
         lib.ref_cb_phantom_volume.argtypes = [_f32p, _f32p, _f32p, _f32p, _f64p]
         lib.ref_aml_ring.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_dbl, _c_dbl, _c_int]
+        lib.ref_high_peaks.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_dbl, _c_int]
+        lib.ref_column_ring.argtypes = [_f32p, _c_int, _c_int, _c_int]
         lib.ref_aml_ring_artefacts.argtypes = [_f32p, _c_int, _c_int, _c_int, ctypes.c_float,
                                                ctypes.c_float, _c_int, _f32p]
         lib.ref_cb_solve_explicit.argtypes = [_c_int] + [_c_dbl] * 4 + [
@@ -470,6 +485,44 @@ def ref_aml_ring_artefacts(pixels, param_n, param_r, num_series):
     with quiet():
         reference().ref_aml_ring_artefacts(pixels, na, nv, nh, float(param_n), float(param_r),
                                            int(num_series), out)
+    return out
+
+
+# ------------------------------------- high-peaks and column ring filters
+def high_peaks(p, jump, num_pix):
+    """The restatement's high-peaks filter on a log sinogram (na, nh, nv);
+    returns the filtered copy (Core/src/diamond.cpp:513-617)."""
+    out = np.array(p, np.float32, order="C")
+    na, nh, nv = out.shape
+    if restate().rs_high_peaks_f32(out, na, nh, nv, float(jump), int(num_pix)):
+        raise ValueError("high peaks filter: parameters out of range")
+    return out
+
+
+def column_ring(p):
+    """The restatement's column ring filter on a log sinogram (na, nh, nv);
+    returns the filtered copy (Core/src/diamond.cpp:619-658)."""
+    out = np.array(p, np.float32, order="C")
+    na, nh, nv = out.shape
+    restate().rs_column_ring_f32(out, na, nh, nv)
+    return out
+
+
+def ref_high_peaks(p, jump, num_pix):
+    """The reference's Diamond::high_peaks_before on (na, nh, nv) logs."""
+    out = np.array(p, np.float32, order="C")
+    na, nh, nv = out.shape
+    with quiet():
+        reference().ref_high_peaks(out, na, nh, nv, float(jump), int(num_pix))
+    return out
+
+
+def ref_column_ring(p):
+    """The reference's remove_column_ring_artefacts on (na, nh, nv) logs."""
+    out = np.array(p, np.float32, order="C")
+    na, nh, nv = out.shape
+    with quiet():
+        reference().ref_column_ring(out, na, nh, nv)
     return out
 
 

@@ -498,6 +498,47 @@ extern "C" void ref_aml_ring(float *p, int na, int nh, int nv, double param_n, d
   std::memcpy(p, px.data(), sizeof(float) * std::size_t(na) * nh * nv);
 }
 
+// The reference's high-peaks filter is a private member of CCPi::Diamond
+// (Core/src/instruments.hpp:371, diamond.cpp:513-617).  An explicit template
+// instantiation may name a private member; it hands the member pointer to a
+// friend function, through which the harness calls the reference's own code
+// on a Diamond whose sizes and pixels it sets.
+struct hp_member {
+  typedef void (CCPi::Diamond::*type)(const real, const int);
+  friend type hp_get(hp_member);
+};
+template <typename Tag, typename Tag::type M> struct hp_expose {
+  friend typename Tag::type hp_get(Tag) { return M; }
+};
+template struct hp_expose<hp_member, &CCPi::Diamond::high_peaks_before>;
+
+class hp_diamond : public CCPi::Diamond {
+public:
+  void load(const float *p, int na, int nh, int nv) {
+    set_phi(na);
+    set_h_pixels(nh);
+    set_v_pixels(nv);
+    pixel_3d &px = create_pixel_data();
+    std::memcpy(px.data(), p, sizeof(float) * std::size_t(na) * nh * nv);
+  }
+};
+
+// CCPi::Diamond::high_peaks_before on a log sinogram [angle][h][v], in place.
+extern "C" void ref_high_peaks(float *p, int na, int nh, int nv, double jump, int num_pix) {
+  hp_diamond d;
+  d.load(p, na, nh, nv);
+  (d.*hp_get(hp_member()))(jump, num_pix);
+  std::memcpy(p, d.get_pixel_data().data(), sizeof(float) * std::size_t(na) * nh * nv);
+}
+
+// CCPi::remove_column_ring_artefacts (diamond.cpp:619-658), in place.
+extern "C" void ref_column_ring(float *p, int na, int nh, int nv) {
+  pixel_data px(boost::extents[na][nh][nv]);
+  std::memcpy(px.data(), p, sizeof(float) * std::size_t(na) * nh * nv);
+  CCPi::remove_column_ring_artefacts(px, na, nh, nv);
+  std::memcpy(p, px.data(), sizeof(float) * std::size_t(na) * nh * nv);
+}
+
 // parallelbeam.filters.aml_ring_artefacts as the reference's wrapper runs it
 // (Wrappers/Python/src/diamond_wrapper.cpp:18-51): pixels (na, nv, nh)
 // transmission in, exp(-filtered -log) out, same layout.

@@ -1258,6 +1258,69 @@ void rs_neglog_f32(const float *in, float *out, long long n) {
   for (long long i = 0; i < n; i++)
     out[i] = -std::log(in[i]);
 }
+
+void rs_expneg_f32(const float *in, float *out, long long n) {
+  for (long long i = 0; i < n; i++)
+    out[i] = std::exp(-in[i]);
+}
+}
+
+// ---------------------------------------------------------------------------
+// High-peaks filter (Core/src/diamond.cpp:513-617).  Per detector row v, and
+// num_pix times: first every angle a < na-1 becomes p[a+1] + d with
+// d = p[a] - p[a+1] raised to -jump when below it (the comparison is FP64,
+// the float difference against the real jump); then, on that result, every
+// angle a+1 > 0 becomes p[a] + d with d = p[a+1] - p[a] limited the same
+// way.  Each pass forms all its differences before it writes (the
+// reference's temp1 plane), which this restatement keeps as written.
+extern "C" int rs_high_peaks_f32(float *p, int na, int nh, int nv, double jump, int num_pix) {
+  if (jump < 0.0 || num_pix < 1 || num_pix >= na)
+    return 1;
+  auto at = [&](int a, int h, int v) -> float & {
+    return p[(size_t(a) * nh + h) * nv + v];
+  };
+  std::vector<float> d(size_t(na - 1) * nh);
+  for (int v = 0; v < nv; v++)
+    for (int k = 0; k < num_pix; k++) {
+      for (int a = 0; a + 1 < na; a++)
+        for (int h = 0; h < nh; h++) {
+          float t = at(a, h, v) - at(a + 1, h, v);
+          if (double(t) < -jump)
+            t = float(-jump);
+          d[size_t(a) * nh + h] = t;
+        }
+      for (int a = 0; a + 1 < na; a++)
+        for (int h = 0; h < nh; h++)
+          at(a, h, v) = at(a + 1, h, v) + d[size_t(a) * nh + h];
+      for (int a = 0; a + 1 < na; a++)
+        for (int h = 0; h < nh; h++) {
+          float t = at(a + 1, h, v) - at(a, h, v);
+          if (double(t) < -jump)
+            t = float(-jump);
+          d[size_t(a) * nh + h] = t;
+        }
+      for (int a = na - 2; a >= 0; a--)
+        for (int h = 0; h < nh; h++)
+          at(a + 1, h, v) = at(a, h, v) + d[size_t(a) * nh + h];
+    }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Column ring-artefact filter (Core/src/diamond.cpp:619-658): per (h, v),
+// the FP64 sum over angles in order, divided by na, rounded to float once
+// and subtracted from every angle.
+extern "C" void rs_column_ring_f32(float *p, int na, int nh, int nv) {
+  for (int v = 0; v < nv; v++)
+    for (int h = 0; h < nh; h++) {
+      double s = 0.0;
+      for (int a = 0; a < na; a++)
+        s += double(p[(size_t(a) * nh + h) * nv + v]);
+      s /= double(na);
+      const float m = float(s);
+      for (int a = 0; a < na; a++)
+        p[(size_t(a) * nh + h) * nv + v] -= m;
+    }
 }
 
 // ---------------------------------------------------------------------------

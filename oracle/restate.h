@@ -63,8 +63,23 @@ void rs_regularize_f64(int alg, int nx, int ny, int nz, const double *a,
 int rs_aml_ring_f32(float *p, int na, int nh, int nv, double param_n,
                     double param_r, int num_series);
 
+/* High-peaks filter (Core/src/diamond.cpp:513-617) on a log sinogram
+ * [angle][h][v], in place: num_pix rounds of a top-to-bottom and a
+ * bottom-to-top pass that limit every drop between neighbouring angles to
+ * jump.  Returns 1 (p unchanged) for the parameters the reference rejects. */
+int rs_high_peaks_f32(float *p, int na, int nh, int nv, double jump,
+                      int num_pix);
+
+/* Column ring-artefact filter (Core/src/diamond.cpp:619-658), in place:
+ * every (h, v) element loses its FP64 mean over the angles. */
+void rs_column_ring_f32(float *p, int na, int nh, int nv);
+
 /* -log(p) with the C library's logf, as the reference's read_scans does. */
 void rs_neglog_f32(const float *in, float *out, long long n);
+
+/* exp(-p) with the C library's expf, as the reference's filter wrapper
+ * turns logs back into transmission (diamond_wrapper.cpp:45-48). */
+void rs_expneg_f32(const float *in, float *out, long long n);
 
 #ifdef __cplusplus
 }

@@ -161,6 +161,7 @@ def main(prefixes=()):
                             cgls3=crec)
 
     out.update(aml_cases())
+    out.update(prefilter_cases())
     if prefixes:
         out = {k: v for k, v in out.items() if k.startswith(tuple(prefixes))}
     for name, d in out.items():
@@ -188,6 +189,30 @@ def aml_cases():
         res = O.ref_aml_ring_artefacts(pixels, pn, pr, ns)
         out[f"aml{idx}"] = dict(pixels=pixels, param_n=np.float32(pn), param_r=np.float32(pr),
                                 num_series=np.array(ns), out=res)
+    return out
+
+
+def prefilter_cases():
+    """The reference's high-peaks filter (Diamond::high_peaks_before) and
+    column ring filter (remove_column_ring_artefacts) on log sinogram
+    stacks (na, nh, nv): a projected phantom with bright single-angle spikes
+    (the peaks) and per-element offsets (the stripes), including an
+    all-zero padding row."""
+    rng = np.random.default_rng(613)
+    out = {}
+    for idx, (n, na, nh, nv, jump, npix) in enumerate(
+            [(24, 60, 32, 3, 0.05, 1), (32, 90, 44, 4, 0.02, 3), (16, 12, 20, 2, 0.0, 11)]):
+        g = O.parallel_geometry((n, n, nv), na, nh)
+        vol = phantom2d(rng, n, nv) * 0.05
+        with O.quiet():
+            sino = O.ref_forward(g, vol)  # (na, nh, nv)
+        sino = sino + (0.03 * rng.standard_normal((1, nh, nv))).astype(np.float32)
+        spikes = rng.random(sino.shape) < 0.02
+        sino = np.where(spikes, sino + rng.uniform(0.5, 2.0, sino.shape), sino).astype(np.float32)
+        sino[:, :, -1] = 0.0
+        out[f"hp{idx}"] = dict(logs=sino, jump=np.array(jump), num_pix=np.array(npix),
+                               out=O.ref_high_peaks(sino, jump, npix))
+        out[f"colring{idx}"] = dict(logs=sino, out=O.ref_column_ring(sino))
     return out
 
 

@@ -70,6 +70,19 @@ def test_wrapper_rejects_bad_inputs():
         alg.grid(0, 4, 4, 0.0, 1)
 
 
+def test_high_peaks_parameters_checked_before_any_device_work():
+    """jump < 0 and num_pix outside [1, n_angles) are errors of the call
+    itself (the reference reports them and leaves the data unfiltered,
+    diamond.cpp:520-527), raised before the filter touches a GPU."""
+    from ccpi.reconstruction.parallelbeam import filters
+    pix = np.full((6, 2, 5), 0.5, np.float32)
+    for jump, npix in [(-0.1, 1), (0.1, 0), (0.1, 6)]:
+        with pytest.raises(RuntimeError, match="high peaks"):
+            filters.high_peaks(pix, jump, npix)
+    with pytest.raises(ValueError):
+        filters.column_ring_artefacts(np.zeros((4, 5)))
+
+
 def test_setup_geometry_dicts():
     from ccpi.reconstruction.parallelbeam import alg
     d = alg.pb_setup_geometry_from_acquisition(np.zeros((91, 8, 160)), np.zeros(91), 0.0, 1)

@@ -121,3 +121,47 @@ def test_aml_restatement_equals_reference(name):
     p = np.ascontiguousarray(O.neglog(d["pixels"]).transpose(0, 2, 1))  # (na, nh, nv)
     assert np.array_equal(O.aml_ring(p, pn, pr, ns), O.ref_aml_ring(p, pn, pr, ns))
     assert np.array_equal(O.ref_aml_ring_artefacts(d["pixels"], pn, pr, ns), d["out"])
+
+
+@pytest.mark.parametrize("name", golden_names("hp"))
+def test_high_peaks_restatement_equals_golden(name):
+    """The restatement of Diamond::high_peaks_before equals the reference's
+    output stored in the fixture, bit for bit (and the reference itself
+    when it is built)."""
+    d = golden(name)
+    jump, npix = float(d["jump"]), int(d["num_pix"])
+    assert np.array_equal(O.high_peaks(d["logs"], jump, npix), d["out"])
+    if O.reference_available():
+        assert np.array_equal(O.ref_high_peaks(d["logs"], jump, npix), d["out"])
+
+
+@pytest.mark.parametrize("name", golden_names("colring"))
+def test_column_ring_restatement_equals_golden(name):
+    d = golden(name)
+    assert np.array_equal(O.column_ring(d["logs"]), d["out"])
+    if O.reference_available():
+        assert np.array_equal(O.ref_column_ring(d["logs"]), d["out"])
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_prefilters_restatement_equal_reference_random(seed):
+    """Random sizes, jumps (zero, tiny, larger than any drop) and rounds up
+    to n_angles - 1 against the reference library."""
+    if not O.reference_available():
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(100 + seed)
+    na, nh, nv = int(rng.integers(2, 40)), int(rng.integers(1, 30)), int(rng.integers(1, 6))
+    p = rng.uniform(-1.0, 3.0, (na, nh, nv)).astype(np.float32)
+    jump = [0.0, 1e-3, 0.3, 1e9][seed]
+    npix = int(rng.integers(1, na))
+    assert np.array_equal(O.high_peaks(p, jump, npix), O.ref_high_peaks(p, jump, npix))
+    assert np.array_equal(O.column_ring(p), O.ref_column_ring(p))
+
+
+def test_high_peaks_restatement_rejects_what_the_reference_rejects():
+    p = np.ones((5, 3, 2), np.float32)
+    for jump, npix in [(-0.1, 1), (0.1, 0), (0.1, 5)]:
+        with pytest.raises(ValueError):
+            O.high_peaks(p, jump, npix)
+        if O.reference_available():  # reported and skipped: data unchanged
+            assert np.array_equal(O.ref_high_peaks(p, jump, npix), p)
