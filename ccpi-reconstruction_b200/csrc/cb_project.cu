@@ -169,6 +169,9 @@ __device__ __forceinline__ float cb_fp_epi(float acc, i64 idx, const Epi &e, dou
 }
 
 constexpr int kFpWarps = 4;
+#ifndef CB_FP_PACKED
+#define CB_FP_PACKED 1
+#endif
 
 // Floats of the slice-plane table copy at the start of the forward
 // projector's shared memory (nz + 1 entries, rounded up to 4).
@@ -283,6 +286,48 @@ __global__ void __launch_bounds__(kFpWarps * 32)
         dk[q] = below[q] ? -1 : 1;
         vzq[q] = svz + (below[q] ? 0 : 1);
       }
+#if CB_FP_PACKED
+      if (FULL) {
+        // rows q and q + 1 as packed pairs: per row the same unfused float
+        // operations as below, two rows per multiply and subtract
+        // instruction; the products only feed scalar adds
+        float2 acc2[RPL / 2], dz2[RPL / 2], iz2[RPL / 2];
+#pragma unroll
+        for (int q = 0; q < RPL; q += 2) {
+          acc2[q / 2] = make_float2(0.0f, 0.0f);
+          dz2[q / 2] = make_float2(dzv[q], dzv[q + 1]);
+          iz2[q / 2] = make_float2(izv[q], izv[q + 1]);
+        }
+        for (int m = 1; m < mfast; m++) {
+          const float a0 = alphas[m - 1], a1 = alphas[m];
+          const int cell = cells[m - 1];
+          if (cell < 0)
+            continue;
+          const float *col = vol + i64(cell) * g.nz;
+          const float av = __fmul_rn(a0, inv_dz);
+          const float2 av2 = make_float2(av, av), a02 = make_float2(a0, a0),
+                       a12 = make_float2(a1, a1);
+#pragma unroll
+          for (int q = 0; q < RPL; q += 2) {
+            const float2 kz = mul2_rn(av2, dz2[q / 2]);
+            const int k0 = int(__fadd_rn(pzbz, kz.x)), k1 = int(__fadd_rn(pzbz, kz.y));
+            const float2 pl = mul2_rn(make_float2(vzq[q][k0], vzq[q + 1][k1]), iz2[q / 2]);
+            const float2 mz = make_float2(fmin_ref(pl.x, a1), fmin_ref(pl.y, a1));
+            const float2 lo = sub2_rn(mz, a02), hi = sub2_rn(a12, mz);
+            const float2 pk = mul2_rn(make_float2(__ldg(col + k0), __ldg(col + k1)), lo);
+            const float2 pn =
+                mul2_rn(make_float2(__ldg(col + k0 + dk[q]), __ldg(col + k1 + dk[q + 1])), hi);
+            acc2[q / 2] = add2_rn(acc2[q / 2],
+                                  make_float2(__fadd_rn(pk.x, pn.x), __fadd_rn(pk.y, pn.y)));
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < RPL; q += 2) {
+          acc[q] = acc2[q / 2].x;
+          acc[q + 1] = acc2[q / 2].y;
+        }
+      } else
+#endif
       for (int m = 1; m < mfast; m++) {
         const float a0 = alphas[m - 1], a1 = alphas[m];
         const int cell = cells[m - 1];
@@ -577,6 +622,9 @@ constexpr int kGaRays = kBpMaxRaysPerAngle; // slots per angle
 #ifndef CB_GA_FAST
 #define CB_GA_FAST 1
 #endif
+#ifndef CB_GA_PACKED
+#define CB_GA_PACKED 1
+#endif
 constexpr int kGaStage = CB_GA_STAGE;
 
 __host__ __device__ inline int round4(int n) { return (n + 3) & ~3; }
@@ -639,6 +687,19 @@ __device__ int cb_ga_stage_rays(const Geom &g, int ac, int nac, double x0, doubl
       map[off[tid] + c] = tid * kGaRays + c;
   __syncthreads();
   return off[nac];
+}
+
+// First-row table: row v of slice k follows row v - 1 of slice kp, so v is
+// the first band row of the slices kp + 1 .. k (entries 0 .. nz + 1 kept).
+__device__ __forceinline__ void cb_ga_mark(int *f, int kp, int k, int v, int nz) {
+#if CB_GA_FAST
+  if (k == kp + 1 && k >= 0 && k <= nz + 1) {
+    f[k] = v; // the usual step: one slice per row change
+    return;
+  }
+#endif
+  for (int K = max(kp + 1, 0); K <= min(k, nz + 1); K++)
+    f[K] = v;
 }
 
 // Register bound: 4 CTAs per SM for one voxel per thread; taller columns
@@ -780,21 +841,50 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
         }
 #endif
         float *c1 = prow + s * prs, *c2 = drow + s * prs;
+#if CB_GA_PACKED
+        const float2 av2 = make_float2(av, av), a02 = make_float2(a0, a0),
+                     a12 = make_float2(a1, a1);
+#endif
 #pragma unroll
         for (int r = 0; r < RMAX; r++) {
+#if CB_GA_PACKED
+          if (r + 1 < RMAX && (r & 1) == 0) {
+            // rows r and r + 1 as packed pairs: the same unfused float
+            // operations per row, two rows per multiply and subtract
+            const int v0 = min_v + tid + r * kGaThreads, v1 = v0 + kGaThreads;
+            const float2 kk = mul2_rn(av2, make_float2(rsd[r], rsd[r + 1]));
+            const float2 kq = mul2_rn(av2, make_float2(rsp[r], rsp[r + 1]));
+            const int k0 = int(__fadd_rn(pzbz, kk.x)), k1 = int(__fadd_rn(pzbz, kk.y));
+            if (v0 < max_v && v0 > min_v)
+              cb_ga_mark(f, int(__fadd_rn(pzbz, kq.x)), k0, v0, nz);
+            if (v1 < max_v)
+              cb_ga_mark(f, int(__fadd_rn(pzbz, kq.y)), k1, v1, nz);
+            const int kz0 = min(max(v0 < mid ? k0 : k0 + 1, 0), nz);
+            const int kz1 = min(max(v1 < mid ? k1 : k1 + 1, 0), nz);
+            const float2 pl =
+                mul2_rn(make_float2(svz[kz0], svz[kz1]), make_float2(rsi[r], rsi[r + 1]));
+            const float2 mz = make_float2(fmin_ref(pl.x, a1), fmin_ref(pl.y, a1));
+            const float2 p = mul2_rn(make_float2(pv[s][r], pv[s][r + 1]),
+                                     make_float2(dv[s][r], dv[s][r + 1]));
+            const float2 w1 = mul2_rn(p, sub2_rn(mz, a02)), w2 = mul2_rn(p, sub2_rn(a12, mz));
+            if (v0 < max_v) {
+              c1[v0] = w1.x;
+              c2[v0] = w2.x;
+            }
+            if (v1 < max_v) {
+              c1[v1] = w1.y;
+              c2[v1] = w2.y;
+            }
+            continue;
+          }
+          if (r & 1)
+            continue; // done with its pair
+#endif
           const int v = min_v + tid + r * kGaThreads;
           if (v < max_v) {
             const int k = int(__fadd_rn(pzbz, __fmul_rn(av, rsd[r])));
-            if (v > min_v) {
-              const int kp = int(__fadd_rn(pzbz, __fmul_rn(av, rsp[r])));
-#if CB_GA_FAST
-              if (k == kp + 1 && k >= 0 && k <= nz + 1)
-                f[k] = v; // the usual step: one slice per row change
-              else
-#endif
-                for (int K = max(kp + 1, 0); K <= min(k, nz + 1); K++)
-                  f[K] = v;
-            }
+            if (v > min_v)
+              cb_ga_mark(f, int(__fadd_rn(pzbz, __fmul_rn(av, rsp[r]))), k, v, nz);
             const int kz = min(max(v < mid ? k : k + 1, 0), nz);
             const float mz = fmin_ref(__fmul_rn(svz[kz], rsi[r]), a1);
             const float p = __fmul_rn(pv[s][r], dv[s][r]);

@@ -72,14 +72,92 @@ enum EpiMode {
 
 __device__ __forceinline__ int warp_lane() { return threadIdx.x & 31; }
 
-// acc += x * w, element-wise, unfused (two roundings per element, as the
-// reference's x86-64 build computes it).  Scalar intrinsics on purpose: the
-// packed f32x2 pair was measured to lose this equality.
-__device__ __forceinline__ void axpy4(float4 &acc, const float4 x, float w) {
+#ifndef CCPI_AXPY_PACKED
+#define CCPI_AXPY_PACKED 1
+#endif
+
+// Blackwell packed FP32 pairs (PTX mul/sub/add.rn.f32x2, sm_100): one
+// instruction rounds both lanes to nearest, each on its own, exactly as two
+// scalar __fmul_rn / __fsub_rn / __fadd_rn would (subnormals kept, no .ftz).
+// One rule keeps them equal to the unfused scalar arithmetic: a packed add
+// or sub never takes a packed product as an operand, because ptxas
+// contracts mul.f32x2 -> add.f32x2 into a fused multiply-add even with
+// explicit rounding.  Products feed scalar adds instead.
+__device__ __forceinline__ float2 mul2_rn(float2 a, float2 b) {
+  float2 r;
+  asm("{ .reg .b64 x, y, z;\n\t"
+      "mov.b64 x, {%2, %3};\n\t"
+      "mov.b64 y, {%4, %5};\n\t"
+      "mul.rn.f32x2 z, x, y;\n\t"
+      "mov.b64 {%0, %1}, z;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 sub2_rn(float2 a, float2 b) {
+  float2 r;
+  asm("{ .reg .b64 x, y, z;\n\t"
+      "mov.b64 x, {%2, %3};\n\t"
+      "mov.b64 y, {%4, %5};\n\t"
+      "sub.rn.f32x2 z, x, y;\n\t"
+      "mov.b64 {%0, %1}, z;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
+  float2 r;
+  asm("{ .reg .b64 x, y, z;\n\t"
+      "mov.b64 x, {%2, %3};\n\t"
+      "mov.b64 y, {%4, %5};\n\t"
+      "add.rn.f32x2 z, x, y;\n\t"
+      "mov.b64 {%0, %1}, z;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
+// (ax, ay) += (xx, xy) * w: the products as one packed multiply, the sums
+// as scalar adds (see above: no packed add of a packed product).
+__device__ __forceinline__ void axpy2_packed(float &ax, float &ay, float xx, float xy, float w) {
+  const float2 p = mul2_rn(make_float2(xx, xy), make_float2(w, w));
+  ax = __fadd_rn(ax, p.x);
+  ay = __fadd_rn(ay, p.y);
+}
+
+// (ax, ay) += (p0, p1) as one packed add (p0, p1 not packed products).
+__device__ __forceinline__ void add2_packed(float &ax, float &ay, float p0, float p1) {
+  const float2 r = add2_rn(make_float2(ax, ay), make_float2(p0, p1));
+  ax = r.x;
+  ay = r.y;
+}
+
+// acc += x * w with scalar products and packed sums (the back projector's
+// form; the forward projector's axpy4 packs the products instead).
+__device__ __forceinline__ void axpy4_pa(float4 &acc, const float4 x, float w) {
+#if CCPI_AXPY_PACKED
+  add2_packed(acc.x, acc.y, __fmul_rn(x.x, w), __fmul_rn(x.y, w));
+  add2_packed(acc.z, acc.w, __fmul_rn(x.z, w), __fmul_rn(x.w, w));
+#else
   acc.x = __fadd_rn(acc.x, __fmul_rn(x.x, w));
   acc.y = __fadd_rn(acc.y, __fmul_rn(x.y, w));
   acc.z = __fadd_rn(acc.z, __fmul_rn(x.z, w));
   acc.w = __fadd_rn(acc.w, __fmul_rn(x.w, w));
+#endif
+}
+
+// acc += x * w, element-wise, unfused (two roundings per element, as the
+// reference's x86-64 build computes it).
+__device__ __forceinline__ void axpy4(float4 &acc, const float4 x, float w) {
+#if CCPI_AXPY_PACKED
+  axpy2_packed(acc.x, acc.y, x.x, x.y, w);
+  axpy2_packed(acc.z, acc.w, x.z, x.w, w);
+#else
+  acc.x = __fadd_rn(acc.x, __fmul_rn(x.x, w));
+  acc.y = __fadd_rn(acc.y, __fmul_rn(x.y, w));
+  acc.z = __fadd_rn(acc.z, __fmul_rn(x.z, w));
+  acc.w = __fadd_rn(acc.w, __fmul_rn(x.w, w));
+#endif
 }
 
 // Deterministic CTA reduction of a double (fixed shuffle/smem order).

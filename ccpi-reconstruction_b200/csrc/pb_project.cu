@@ -850,7 +850,7 @@ __global__ void __launch_bounds__(256, NP * VW <= 16 ? 4 : (NP * VW <= 32 ? 3 : 
             x[f] = __ldg(p + f * nzg);
 #pragma unroll
           for (int f = 0; f < NF; f++)
-            axpy4(acc[k][f], x[f], w);
+            axpy4_pa(acc[k][f], x[f], w);
         }
       }
     }
