@@ -753,6 +753,18 @@ def main():
     t_bp = e0.elapsed_time(e1) / 1000.0 / reps
     del tmp_p, tmp_v
 
+    # ---- the projectors' own ceiling: random whole-column reads from an
+    # L2-resident 64 MiB set (ccpi_measure_gather), outside the timed region.
+    # Each ray-cell visit of the FP (and each column-ray pair of the BP)
+    # moves one nz-float column; for unit pixels and voxels the visits of one
+    # angle are nx * ny * (|cos| + |sin|), so one projection gathers
+    # 4 V sum_a (|cos a| + |sin a|) bytes.
+    gather_peak = np.zeros(1, np.float64)
+    N.check(N.lib.ccpi_measure_gather(64 << 20, ctypes.c_void_p(stream.cuda_stream), gather_peak),
+            "ccpi_measure_gather")
+    ang_rad = np.asarray(plan._arrays[0], np.float64)
+    gather_bytes = 4.0 * V * float(np.sum(np.abs(np.cos(ang_rad)) + np.abs(np.sin(ang_rad))))
+
     # ---- plain: one slice per launch sequence, host-driven iterations
     plain = None
     if not args.no_plain:
@@ -840,6 +852,15 @@ def main():
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "traffic": load_traffic()},
+            "gather_roofline": {
+                "bound": "L2 -> SM gathers", "unit": "GB/s",
+                "peak": float(gather_peak[0]),
+                "peak_kind": "measured live: ccpi_measure_gather, random 1 KB columns, 64 MiB set",
+                "bytes_per_launch": gather_bytes,
+                "fp": {"achieved": gather_bytes / t_fp / 1e9,
+                       "frac": gather_bytes / t_fp / 1e9 / float(gather_peak[0])},
+                "bp": {"achieved": gather_bytes / t_bp / 1e9,
+                       "frac": gather_bytes / t_bp / 1e9 / float(gather_peak[0])}},
             "e2e": {"value": world * e2e_it / t_e2e, "unit": "iter/s",
                     "h2d_bytes_per_step": host_in.numel() * 4 / e2e_it,
                     "d2h_bytes_per_step": host_out.numel() * 4 / e2e_it,

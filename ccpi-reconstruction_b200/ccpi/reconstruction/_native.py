@@ -59,6 +59,7 @@ def _load():
                                        _f32p]
     lib.ccpi_pb_column_ring_artefacts.argtypes = [_f32p, _c_int, _c_int, _c_int, _c_int, _f32p]
     lib.ccpi_high_peaks.argtypes = [_vp, _c_int, _c_int, _c_int, _c_dbl, _c_int, _vp]
+    lib.ccpi_measure_gather.argtypes = [ctypes.c_ulonglong, _vp, _f64p]
     lib.ccpi_ring_filter_column.argtypes = [_vp, _c_int, _c_int, _c_int, _vp]
     lib.ccpi_pb_forward_project.argtypes = [_f32p, _c_int, _c_int, _c_int, _f32p, _c_int,
                                             _c_int, _vp, _i32p]

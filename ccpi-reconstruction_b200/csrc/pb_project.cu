@@ -547,54 +547,7 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
           const int nj = __shfl_sync(0xffffffffu, n, jj);
           const uint2 *cl = S.cell + jj * kSlotCap;
           int m = 0;
-#if PB_FP_BATCH == 8
-          for (; m + 8 <= nj; m += 8) {
-            const uint4 p0 = *reinterpret_cast<const uint4 *>(cl + m);
-            const uint4 p1 = *reinterpret_cast<const uint4 *>(cl + m + 2);
-            const uint4 p2 = *reinterpret_cast<const uint4 *>(cl + m + 4);
-            const uint4 p3 = *reinterpret_cast<const uint4 *>(cl + m + 6);
-            const unsigned o[8] = {p0.x, p0.z, p1.x, p1.z, p2.x, p2.z, p3.x, p3.z};
-            const float l[8] = {__uint_as_float(p0.y), __uint_as_float(p0.w),
-                                __uint_as_float(p1.y), __uint_as_float(p1.w),
-                                __uint_as_float(p2.y), __uint_as_float(p2.w),
-                                __uint_as_float(p3.y), __uint_as_float(p3.w)};
-            float4 xv[8][NQ];
-#pragma unroll
-            for (int u = 0; u < 8; u++)
-#pragma unroll
-              for (int q = 0; q < NQ; q++)
-                if (vok[q])
-                  xv[u][q] = __ldg(vb + o[u] + q * 32);
-#pragma unroll
-            for (int u = 0; u < 8; u++)
-#pragma unroll
-              for (int q = 0; q < NQ; q++)
-                if (vok[q])
-                  axpy4(acc[q], xv[u][q], l[u]);
-          }
-          if (m + 4 <= nj) {
-            const uint4 p0 = *reinterpret_cast<const uint4 *>(cl + m);
-            const uint4 p1 = *reinterpret_cast<const uint4 *>(cl + m + 2);
-            const unsigned o[4] = {p0.x, p0.z, p1.x, p1.z};
-            const float l[4] = {__uint_as_float(p0.y), __uint_as_float(p0.w),
-                                __uint_as_float(p1.y), __uint_as_float(p1.w)};
-            float4 xv[4][NQ];
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-#pragma unroll
-              for (int q = 0; q < NQ; q++)
-                if (vok[q])
-                  xv[u][q] = __ldg(vb + o[u] + q * 32);
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-#pragma unroll
-              for (int q = 0; q < NQ; q++)
-                if (vok[q])
-                  axpy4(acc[q], xv[u][q], l[u]);
-            m += 4;
-          }
-          {
-#elif PB_FP_BATCH == 4
+#if PB_FP_BATCH == 4
           for (; m + 4 <= nj; m += 4) {
             const uint4 p0 = *reinterpret_cast<const uint4 *>(cl + m);
             const uint4 p1 = *reinterpret_cast<const uint4 *>(cl + m + 2);
@@ -607,7 +560,6 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
             const unsigned o[2] = {p0.x, p0.z};
             const float l[2] = {__uint_as_float(p0.y), __uint_as_float(p0.w)};
 #endif
-#if PB_FP_BATCH != 8
             float4 xv[PB_FP_BATCH][NQ];
 #pragma unroll
             for (int u = 0; u < PB_FP_BATCH; u++)
@@ -621,7 +573,6 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
               for (int q = 0; q < NQ; q++)
                 if (vok[q])
                   axpy4(acc[q], xv[u][q], l[u]);
-#endif
           }
           for (; m < nj; m++) {
             const uint2 p = cl[m];

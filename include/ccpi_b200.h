@@ -240,6 +240,16 @@ void ccpi_plan_destroy(ccpi_plan *plan);
  * (may be NULL) receives {grid or rows per lane, slices per lane or 0}.
  * Allocates and frees scratch of one volume and one sinogram. */
 int ccpi_plan_autotune(ccpi_plan *plan, void *stream, int chosen[2]);
+
+/* Measured ceiling of the projectors' gathers: GB/s at which the GPU reads
+ * whole 1 KB columns at random offsets out of a working set of
+ * working_set_bytes (rounded down to a power of two; pick one that fits L2,
+ * e.g. 64 MiB), eight columns in
+ * flight per lane.  A roofline denominator for ray-driven kernels whose
+ * traffic is L2 -> SM rather than HBM.  No counterpart in the reference.
+ * Allocates and frees the working set; waits for `stream`. */
+int ccpi_measure_gather(unsigned long long working_set_bytes, void *stream,
+                        double *gbs);
 /* Sizes of a plan's volume and sinogram in elements. */
 long long ccpi_plan_voxels(const ccpi_plan *plan);
 long long ccpi_plan_pixels(const ccpi_plan *plan);

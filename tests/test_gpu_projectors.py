@@ -164,3 +164,18 @@ def test_create_phantom_like_reference_test(cuda):
     assert data[4] == 0.390625 and data[5] == 0.390625
     assert data[6] == 25.151547886198443
     assert np.isfinite(data[0]).all() and data[0].min() >= 0.0 and data[0].max() > 0.0
+
+
+def test_gather_probe_reports_a_bandwidth(cuda):
+    """ccpi_measure_gather (the projectors' L2 gather ceiling that bench.py
+    reports) runs and returns a plausible figure."""
+    import ctypes
+
+    import numpy as np
+    import torch
+    from ccpi.reconstruction import _native as N
+    out = np.zeros(1, np.float64)
+    st = ctypes.c_void_p(torch.cuda.current_stream(cuda).cuda_stream)
+    N.check(N.lib.ccpi_measure_gather(8 << 20, st, out), "ccpi_measure_gather")
+    assert 100.0 < out[0] < 1e5
+    assert N.lib.ccpi_measure_gather(16, st, out) == 1
