@@ -68,6 +68,8 @@ enum EpiMode {
   EPI_NORM = 1,  // out = A x, and per-CTA sum of squares in FP64
   EPI_SIRT = 2,  // fp: r = (b - Ax) R       bp: x = max(x + C A^T r, 0)
   EPI_MLEM = 3,  // fp: q = max(b / Ax, 0)   bp: x = max(x (N A^T q), 0)
+  EPI_ONES = 4,  // the input is all ones: out = A 1 or A^T 1 (no input read;
+                 // 1 * l == l exactly, so the sums are those of a ones input)
 };
 
 __device__ __forceinline__ int warp_lane() { return threadIdx.x & 31; }
@@ -158,6 +160,14 @@ __device__ __forceinline__ void axpy4(float4 &acc, const float4 x, float w) {
   acc.z = __fadd_rn(acc.z, __fmul_rn(x.z, w));
   acc.w = __fadd_rn(acc.w, __fmul_rn(x.w, w));
 #endif
+}
+
+// acc += 1 * l for a ones input: the product is l exactly, so only the sums.
+__device__ __forceinline__ void add_len4(float4 &acc, float l) {
+  acc.x = __fadd_rn(acc.x, l);
+  acc.y = __fadd_rn(acc.y, l);
+  acc.z = __fadd_rn(acc.z, l);
+  acc.w = __fadd_rn(acc.w, l);
 }
 
 // Deterministic CTA reduction of a double (fixed shuffle/smem order).

@@ -428,6 +428,31 @@ int iterate(const ccpi_plan *p, int alg, const float *sino, float *x, const Work
   return rc;
 }
 
+// pix = A 1 and vol = A^T 1.  The parallel projectors have a form that reads
+// no input (EPI_ONES); elsewhere a ones array is written into the scratch
+// buffer and projected.
+int forward_ones(const ccpi_plan *p, float *scratch_vol, float *pix, cudaStream_t st) {
+  const Epi e{};
+  if (p->g.kind == CCPI_PARALLEL) {
+    const int rc = forward(p, nullptr, pix, EPI_ONES, e, st);
+    if (rc != 3)
+      return rc;
+  }
+  k_fill(scratch_vol, p->nvox, 1.0f, st);
+  return forward(p, scratch_vol, pix, EPI_STORE, e, st);
+}
+
+int backward_ones(const ccpi_plan *p, float *scratch_pix, float *vol, cudaStream_t st) {
+  const Epi e{};
+  if (p->g.kind == CCPI_PARALLEL) {
+    const int rc = backward(p, nullptr, vol, EPI_ONES, e, st);
+    if (rc != 3)
+      return rc;
+  }
+  k_fill(scratch_pix, p->npix, 1.0f, st);
+  return backward(p, scratch_pix, vol, EPI_STORE, e, st);
+}
+
 // Set-up before the first iteration (kernels only).
 int prepare(const ccpi_plan *p, int alg, const float *sino, float *x, const Work &W,
             cudaStream_t st) {
@@ -449,18 +474,15 @@ int prepare(const ccpi_plan *p, int alg, const float *sino, float *x, const Work
     break;
   case CCPI_SIRT:
     // R = 1 / (A 1), C = 1 / (A^T 1), non-positive -> 0 (sirt.cpp:31-48)
-    k_fill(W.d, V, 1.0f, st);
-    rc |= forward(p, W.d, W.q, EPI_STORE, e, st);
+    rc |= forward_ones(p, W.d, W.q, st);
     k_invert_pos(W.q, P, st);
-    k_fill(W.r, P, 1.0f, st);
-    rc |= backward(p, W.r, W.d, EPI_STORE, e, st);
+    rc |= backward_ones(p, W.r, W.d, st);
     k_invert_pos(W.d, V, st);
     break;
   case CCPI_MLEM:
     // x = 1; N = 1 / (A^T 1), zeros kept (mlem.cpp:30-41)
     k_fill(x, V, 1.0f, st);
-    k_fill(W.r, P, 1.0f, st);
-    rc |= backward(p, W.r, W.d, EPI_STORE, e, st);
+    rc |= backward_ones(p, W.r, W.d, st);
     k_invert_nonzero(W.d, V, st);
     break;
   default:

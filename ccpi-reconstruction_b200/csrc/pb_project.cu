@@ -560,26 +560,40 @@ __global__ void __launch_bounds__(kLaneWarps * 32, PB_FP_MINB)
             const unsigned o[2] = {p0.x, p0.z};
             const float l[2] = {__uint_as_float(p0.y), __uint_as_float(p0.w)};
 #endif
-            float4 xv[PB_FP_BATCH][NQ];
+            if (EPI == EPI_ONES) {
+              (void)o;
 #pragma unroll
-            for (int u = 0; u < PB_FP_BATCH; u++)
+              for (int u = 0; u < PB_FP_BATCH; u++)
 #pragma unroll
-              for (int q = 0; q < NQ; q++)
-                if (vok[q])
-                  xv[u][q] = __ldg(vb + o[u] + q * 32);
+                for (int q = 0; q < NQ; q++)
+                  if (vok[q])
+                    add_len4(acc[q], l[u]);
+            } else {
+              float4 xv[PB_FP_BATCH][NQ];
 #pragma unroll
-            for (int u = 0; u < PB_FP_BATCH; u++)
+              for (int u = 0; u < PB_FP_BATCH; u++)
 #pragma unroll
-              for (int q = 0; q < NQ; q++)
-                if (vok[q])
-                  axpy4(acc[q], xv[u][q], l[u]);
+                for (int q = 0; q < NQ; q++)
+                  if (vok[q])
+                    xv[u][q] = __ldg(vb + o[u] + q * 32);
+#pragma unroll
+              for (int u = 0; u < PB_FP_BATCH; u++)
+#pragma unroll
+                for (int q = 0; q < NQ; q++)
+                  if (vok[q])
+                    axpy4(acc[q], xv[u][q], l[u]);
+            }
           }
           for (; m < nj; m++) {
             const uint2 p = cl[m];
 #pragma unroll
             for (int q = 0; q < NQ; q++)
-              if (vok[q])
-                axpy4(acc[q], __ldg(vb + p.x + q * 32), __uint_as_float(p.y));
+              if (vok[q]) {
+                if (EPI == EPI_ONES)
+                  add_len4(acc[q], __uint_as_float(p.y));
+                else
+                  axpy4(acc[q], __ldg(vb + p.x + q * 32), __uint_as_float(p.y));
+              }
           }
         }
         __syncwarp();
@@ -844,13 +858,20 @@ __global__ void __launch_bounds__(256, NP * VW <= 16 ? 4 : (NP * VW <= 32 ? 3 : 
         for (int r = 0; r < cnt; r++) {
           const float w = E[ai].w[r];
           const float4 *p = reinterpret_cast<const float4 *>(base + i64(row0 + r) * g.nv);
-          float4 x[NF];
+          if (EPI == EPI_ONES) {
+            (void)p;
 #pragma unroll
-          for (int f = 0; f < NF; f++)
-            x[f] = __ldg(p + f * nzg);
+            for (int f = 0; f < NF; f++)
+              add_len4(acc[k][f], w);
+          } else {
+            float4 x[NF];
 #pragma unroll
-          for (int f = 0; f < NF; f++)
-            axpy4_pa(acc[k][f], x[f], w);
+            for (int f = 0; f < NF; f++)
+              x[f] = __ldg(p + f * nzg);
+#pragma unroll
+            for (int f = 0; f < NF; f++)
+              axpy4_pa(acc[k][f], x[f], w);
+          }
         }
       }
     }
@@ -954,16 +975,19 @@ __global__ void __launch_bounds__(256) pb_bp_scalar(Geom g, const float *__restr
     store_partial<8>(ssq, e);
 }
 
+// The lane-parallel forward kernel applies: row v <-> slice v, float4 rows,
+// float4 offsets of the columns fit 32 bits, and a ray's block list (at most
+// about nbx + nby entries) fits its staging area.
+bool pb_fp_vec4(const Geom &g) {
+  const int nblocks = (g.nx + kBlock - 1) / kBlock + (g.ny + kBlock - 1) / kBlock;
+  return g.map_type == 1 && (g.nv % 4) == 0 && (g.nz % 4) == 0 &&
+         (long long)g.nx * g.ny * (g.nz / 4) < (1ll << 32) && nblocks + 16 <= kMaxBlocks;
+}
+
 template <int EPI>
 int launch_fp(const Geom &g, const float *vol, float *pix, const Epi &e, int grid, int *err,
               cudaStream_t st) {
-  // float4 offsets of the columns must fit 32 bits, and a ray's block list
-  // (at most about nbx + nby entries) must fit its staging area
-  const int nblocks = (g.nx + kBlock - 1) / kBlock + (g.ny + kBlock - 1) / kBlock;
-  const bool vec4 = g.map_type == 1 && (g.nv % 4) == 0 && (g.nz % 4) == 0 &&
-                    (long long)g.nx * g.ny * (g.nz / 4) < (1ll << 32) &&
-                    nblocks + 16 <= kMaxBlocks;
-  if (vec4) {
+  if (pb_fp_vec4(g)) {
     const size_t smem = sizeof(LaneSmem) * kLaneWarps;
     for (int v0 = 0; v0 < g.nv; v0 += 256) {
       if (g.nv - v0 > 128)
@@ -971,7 +995,7 @@ int launch_fp(const Geom &g, const float *vol, float *pix, const Epi &e, int gri
       else
         pb_fp_lanes<1, EPI><<<grid, kLaneWarps * 32, smem, st>>>(g, vol, pix, e, v0, err);
     }
-  } else {
+  } else if (EPI != EPI_ONES) {
     for (int v0 = 0; v0 < g.nv; v0 += 256) {
       const int left = g.nv - v0;
       if (left > 128)
@@ -1045,7 +1069,7 @@ int launch_bp_np(const Geom &g, const BpShape &b, const float *pix, float *vol, 
     pb_bp_vec<NP, 8, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
   else if (b.vw == 4)
     pb_bp_vec<NP, 4, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
-  else
+  else if (EPI != EPI_ONES)
     pb_bp_scalar<NP, EPI><<<tiles, 256, smem, st>>>(g, pix, vol, e, b.tw, b.th, err);
   return 0;
 }
@@ -1074,6 +1098,10 @@ int launch_bp(const Geom &g, const float *pix, float *vol, const Epi &e, int *er
 int pb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
                int grid, int *err, cudaStream_t st) {
   switch (mode) {
+  case EPI_ONES:
+    if (!pb_fp_vec4(g))
+      return 3; // no ones form for this geometry: the caller projects a ones volume
+    return launch_fp<EPI_ONES>(g, vol, pix, e, grid, err, st);
   case EPI_STORE:
     return launch_fp<EPI_STORE>(g, vol, pix, e, grid, err, st);
   case EPI_NORM:
@@ -1093,7 +1121,8 @@ int pb_prepare() {
   const void *fns[] = {(const void *)pb_fp_lanes<1, EPI_STORE>, (const void *)pb_fp_lanes<2, EPI_STORE>,
                        (const void *)pb_fp_lanes<1, EPI_NORM>,  (const void *)pb_fp_lanes<2, EPI_NORM>,
                        (const void *)pb_fp_lanes<1, EPI_SIRT>,  (const void *)pb_fp_lanes<2, EPI_SIRT>,
-                       (const void *)pb_fp_lanes<1, EPI_MLEM>,  (const void *)pb_fp_lanes<2, EPI_MLEM>};
+                       (const void *)pb_fp_lanes<1, EPI_MLEM>,  (const void *)pb_fp_lanes<2, EPI_MLEM>,
+                       (const void *)pb_fp_lanes<1, EPI_ONES>,  (const void *)pb_fp_lanes<2, EPI_ONES>};
   for (const void *f : fns)
     if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
       return 1;
@@ -1108,6 +1137,10 @@ int pb_fp_ctas(const Geom &g) {
 int pb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
                 int *err, cudaStream_t st) {
   switch (mode) {
+  case EPI_ONES:
+    if (bp_shape(g).vw < 4)
+      return 3; // no ones form for this geometry: the caller projects a ones sinogram
+    return launch_bp<EPI_ONES>(g, pix, vol, e, err, st);
   case EPI_STORE:
     return launch_bp<EPI_STORE>(g, pix, vol, e, err, st);
   case EPI_NORM:
