@@ -813,12 +813,18 @@ def main():
     N.check(N.lib.ccpi_pb_reconstruct(N.SIRT, host_in.numpy(), NA, NV, NH, ang32, 0.0, 1, 1, 1,
                                       1, 0.0, None, None, host_out.numpy()),
             "ccpi_pb_reconstruct")
-    barrier()
-    t0 = time.perf_counter()
-    rc = N.lib.ccpi_pb_reconstruct(N.SIRT, host_in.numpy(), NA, NV, NH, ang32, 0.0, 1, e2e_it, 1,
-                                   1, 0.0, None, None, host_out.numpy())
-    t_e2e = max_over_ranks(time.perf_counter() - t0)
-    N.check(rc, "ccpi_pb_reconstruct")
+    # three timed calls, the median reported: a single wall-clock call on a
+    # shared host now and then takes several hundred ms longer for reasons
+    # outside the call (seen in traces where every phase but one was steady)
+    e2e_runs = []
+    for _ in range(3):
+        barrier()
+        t0 = time.perf_counter()
+        rc = N.lib.ccpi_pb_reconstruct(N.SIRT, host_in.numpy(), NA, NV, NH, ang32, 0.0, 1,
+                                       e2e_it, 1, 1, 0.0, None, None, host_out.numpy())
+        e2e_runs.append(max_over_ranks(time.perf_counter() - t0))
+        N.check(rc, "ccpi_pb_reconstruct")
+    t_e2e = sorted(e2e_runs)[1]
 
     # ---- CPU baseline (rank 0, N = 1 only)
     cpu = None
@@ -864,7 +870,9 @@ def main():
             "e2e": {"value": world * e2e_it / t_e2e, "unit": "iter/s",
                     "h2d_bytes_per_step": host_in.numel() * 4 / e2e_it,
                     "d2h_bytes_per_step": host_out.numel() * 4 / e2e_it,
-                    "call": "ccpi_pb_reconstruct(SIRT, %d iterations), pinned host buffers" % e2e_it},
+                    "call": "ccpi_pb_reconstruct(SIRT, %d iterations), pinned host buffers; "
+                            "median of 3 timed calls" % e2e_it,
+                    "calls_s": e2e_runs},
             "gpu_launches": 2 * args.steps,
             "clocks": clk,
             "cpu_baseline": cpu,
