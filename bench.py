@@ -67,14 +67,15 @@ def parse():
     return args
 
 
-def load_traffic():
-    """DRAM bytes per launch of the dominant kernel on this workload, from
-    one ncu capture of the same command (1-pass metrics, full size)."""
+def load_traffic(kernel):
+    """DRAM bytes per launch of `kernel` ("pb_fp" or "pb_bp") on this
+    workload, from one ncu capture of the same command (1-pass metrics, full
+    size)."""
     if globals().get("NH") != 768:
         return None
     try:
         with open(os.path.join(ROOT, "profiles", "pb_traffic_768x768x256.json")) as f:
-            return float(json.load(f)["dram_bytes_per_launch"])
+            return float(json.load(f)["kernels"][kernel]["dram_bytes_per_launch"])
     except Exception:
         return None
 
@@ -857,7 +858,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "traffic": load_traffic()},
+                         "traffic": load_traffic(dom.split(" ")[0])},
             "gather_roofline": {
                 "bound": "L2 -> SM gathers", "unit": "GB/s",
                 "peak": float(gather_peak[0]),
