@@ -260,3 +260,42 @@ def test_autotuned_plan_gives_the_same_results(kind, cuda):
             assert torch.equal(xa, xb)
         else:
             assert rel_l2(xb.cpu().numpy(), xa.cpu().numpy()) <= 1e-6
+
+
+def test_sirt_full_size_slices_equal_single_slice_solves(cuda):
+    """The bench workload's size (768x768x256 grid, 720 angles, 768
+    columns): SIRT on all 256 slices at once (the lane-parallel float4
+    kernels) equals, bit for bit, SIRT on one slice at a time (a one-slice
+    plan takes the scalar kernels) for slices at both ends and inside.
+    Parallel-beam SIRT is separable by slice, so any difference would be a
+    kernel error."""
+    import torch
+    from ccpi.reconstruction.device import parallel_plan
+    p = parallel_plan((768, 768, 256), 720, 768)
+    g = torch.Generator(device="cuda").manual_seed(21)
+    s = torch.rand(p.sino_shape, device=cuda, generator=g) * 4.0
+    full = torch.zeros(p.shape, device=cuda)
+    p.solve(1, s, full, 2)
+    p1 = parallel_plan((768, 768, 1), 720, 768)
+    for k in (0, 97, 255):
+        xk = torch.zeros(p1.shape, device=cuda)
+        p1.solve(1, s[:, :, k:k + 1].contiguous(), xk, 2)
+        assert torch.equal(xk[:, :, 0], full[:, :, k]), k
+
+
+def test_cone_full_size_linearity(cuda):
+    """The 512^3 cone workload (720 angles, 768^2 detector): A(2x) == 2 A(x)
+    and A^T(2y) == 2 A^T(y) exactly (scaling by 2 is exact in float), and
+    every value finite."""
+    import torch
+    from ccpi.reconstruction.device import cone_plan
+    p = cone_plan(512, 1.0, 720, 768, 0.8, 500.0, 500.0)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.rand(p.shape, device=cuda, generator=g)
+    a1 = p.forward(x)
+    assert torch.equal(p.forward(2 * x), 2 * a1)
+    assert torch.isfinite(a1).all()
+    del x
+    b1 = p.backward(a1)
+    assert torch.equal(p.backward(2 * a1), 2 * b1)
+    assert torch.isfinite(b1).all()
