@@ -71,6 +71,7 @@ def _load():
     lib.ccpi_cb_reconstruct.argtypes = [_c_int, _f32p, _c_int, _c_int, _c_int, _f32p, _c_int] + \
         [_c_dbl] * 5 + [_c_int, _c_int, _c_int, _c_dbl, _vp, _f32p]
     lib.ccpi_cb_create_sinogram.argtypes = [P(Geometry), _f32p, _f32p]
+    lib.ccpi_reconstruct.argtypes = [P(Geometry), _c_int, _vp, _c_int, _c_dbl, _vp, _vp]
     lib.ccpi_plan_create.argtypes = [P(Geometry), P(_vp)]
     lib.ccpi_plan_autotune.argtypes = [_vp, _vp, _i32p]
     lib.ccpi_plan_destroy.argtypes = [_vp]

@@ -173,6 +173,46 @@ def create_sinogram(source_x, source_y, source_z, detector_x, h_pixels, v_pixels
     return out
 
 
+def reconstruct_explicit(algorithm, source, detector_x, h_pixels, v_pixels, angles, sino,
+                         grid_offset, voxel_size, shape, niterations, regularize=0.0,
+                         norm_r=None):
+    """A cone-beam solver on an explicit geometry with host arrays
+    (``ccpi_reconstruct``; the reference's reconstruction_alg::reconstruct
+    on an explicitly set instrument, Core/src/algorithms.hpp:13-20).
+    algorithm: "cgls", "sirt", "mlem", "cgls_tikhonov" or "cgls_TVreg";
+    angles in radians; sino (n_angles, n_h, n_v) log data; returns the
+    clamped volume of `shape`; norm_r (optional, one entry per iteration)
+    receives |A^T r| for the CGLS family."""
+    algs = {"cgls": N.CGLS, "sirt": N.SIRT, "mlem": N.MLEM, "cgls_tikhonov": N.CGLS_TIKHONOV,
+            "cgls_TVreg": N.CGLS_TV}
+    if algorithm not in algs:
+        raise ValueError(f"unknown algorithm {algorithm!r}")
+    a, h, v = (np.ascontiguousarray(x, np.float64) for x in (angles, h_pixels, v_pixels))
+    s = N.f32(sino, "sino", 3)
+    if s.shape != (len(a), len(h), len(v)):
+        raise ValueError(f"sino has shape {s.shape}, the geometry needs "
+                         f"{(len(a), len(h), len(v))}")
+    g = N.Geometry()
+    g.kind = N.CONE
+    g.angles, g.h_pixels, g.v_pixels = a.ctypes.data, h.ctypes.data, v.ctypes.data
+    g.n_angles, g.n_h, g.n_v = len(a), len(h), len(v)
+    g.source = (ctypes.c_double * 3)(*(float(x) for x in source))
+    g.detector_x = float(detector_x)
+    g.origin = (ctypes.c_double * 3)(*(float(x) for x in grid_offset))
+    g.voxel_size = (ctypes.c_double * 3)(*(float(x) for x in voxel_size))
+    g.nx, g.ny, g.nz = (int(x) for x in shape)
+    out = np.zeros(tuple(int(x) for x in shape), np.float32)
+    norms = np.zeros(max(int(niterations), 1), np.float64)
+    N.check(N.lib.ccpi_reconstruct(ctypes.byref(g), algs[algorithm], s.ctypes.data,
+                                   int(niterations), float(regularize), norms.ctypes.data,
+                                   out.ctypes.data), "reconstruct_explicit")
+    if norm_r is not None:
+        nr = np.asarray(norm_r)
+        n = min(int(niterations), nr.shape[0])
+        nr[:n] = norms[:n]
+    return out
+
+
 # ---- demonstration phantom of the Nikon XTek instrument
 # (Nikon_XTek::create_phantom / build_phantom / initialise_phantom_volume,
 # Core/src/Readers/xtek.cpp:131-175, :392-457, :825-894; wrappers

@@ -82,7 +82,8 @@ extern "C" int ccpi_measure_gather(unsigned long long working_set_bytes, void *s
     return 1;
   }
   const unsigned mask = unsigned(ncols - 1);
-  const int grid = 148 * 4;
+  // four CTAs per SM of the current device (148 SMs on a B200)
+  const int grid = sm_count() * 4;
   float4 *cols = nullptr;
   float *out = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -793,6 +793,39 @@ int ccpi_cb_create_sinogram(const ccpi_geometry *geometry, const float *volume, 
   return 0;
 }
 
+int ccpi_reconstruct(const ccpi_geometry *geometry, int alg, const float *sino, int niter,
+                     double regularize, double *norms, float *volume) {
+  ccpi::g_last_error.clear();
+  if (!geometry || !sino || !volume) {
+    set_error("ccpi_reconstruct: need a geometry and host buffers");
+    return 1;
+  }
+  if (alg < CCPI_CGLS || alg > CCPI_CGLS_TV || niter < 0) {
+    set_error("ccpi_reconstruct: unknown algorithm or negative iteration count");
+    return 1;
+  }
+  PlanHolder P;
+  if (ccpi::plan_create(geometry, &P.p))
+    return 2;
+  const i64 V = P.p->nvox, Pn = P.p->npix;
+  DevBuf dsino, dx;
+  if (!dsino.alloc(Pn * 4) || !dx.alloc(V * 4))
+    return 2;
+  cudaStream_t st = 0;
+  if (!ccpi::cuda_ok(cudaMemcpyAsync(dsino.p, sino, Pn * 4, cudaMemcpyHostToDevice, st),
+                     "ccpi_reconstruct: upload sinogram"))
+    return 2;
+  cudaMemsetAsync(dx.p, 0, V * 4, st);
+  const int rc =
+      ccpi::solve(P.p, alg, dsino.f(), dx.f(), niter, regularize, norms, 0, nullptr, 0, st);
+  if (rc)
+    return rc;
+  if (!ccpi::cuda_ok(cudaMemcpy(volume, dx.p, V * 4, cudaMemcpyDeviceToHost),
+                     "ccpi_reconstruct: download volume"))
+    return 2;
+  return 0;
+}
+
 int ccpi_plan_create(const ccpi_geometry *geometry, ccpi_plan **plan) {
   ccpi::g_last_error.clear();
   if (!plan) {

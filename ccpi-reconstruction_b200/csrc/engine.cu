@@ -32,7 +32,20 @@ bool cuda_ok(cudaError_t e, const char *what) {
   if (e == cudaSuccess)
     return true;
   set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  // the failure is reported through the status and ccpi_last_error(); clear
+  // the runtime's last-error slot so that a recoverable failure (an
+  // allocation refused for lack of memory) does not surface later in the
+  // caller's own error checks
+  cudaGetLastError();
   return false;
+}
+
+int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+    return 148;
+  return n;
 }
 
 namespace {

@@ -24,6 +24,8 @@ namespace ccpi {
 extern thread_local std::string g_last_error;
 void set_error(const std::string &m);
 bool cuda_ok(cudaError_t e, const char *what);
+// Streaming multiprocessors of the current device (148 on a B200).
+int sm_count();
 
 int plan_create(const ccpi_geometry *g, ccpi_plan **out);
 int forward(const ccpi_plan *p, const float *vol, float *pix, int mode, const Epi &e,

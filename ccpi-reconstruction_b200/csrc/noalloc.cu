@@ -85,6 +85,14 @@ extern "C" int ccpi_solve_noalloc(const ccpi_plan *plan, int alg, const float *d
     ccpi::set_error("ccpi_solve_noalloc: no usable current device");
     return 2;
   }
+  // the scratch used is the current device's: it must be the plan's device,
+  // where the plan's tables and the caller's buffers live
+  if (device != plan->device) {
+    ccpi::set_error("ccpi_solve_noalloc: the current device (" + std::to_string(device) +
+                    ") is not the plan's device (" + std::to_string(plan->device) +
+                    "); make the plan's device current first");
+    return 1;
+  }
   void *scratch = static_scratch(device);
   if (!scratch)
     return 2;

@@ -218,6 +218,17 @@ int ccpi_cb_reconstruct(int alg, const float *pixels, int n_angles, int n_h,
 int ccpi_cb_create_sinogram(const ccpi_geometry *geometry,
                             const float *volume, float *out);
 
+/* A solver on an explicit geometry with host buffers: the reference's core
+ * call reconstruction_alg::reconstruct (Core/src/algorithms.hpp:13-20) on an
+ * instrument whose geometry is set explicitly (as its Avizo and Matlab
+ * front-ends do, Wrappers/Avizo/src/CCPiReconstruction/Cone_Beam_recon.cpp:
+ * 114-180), followed by the clamp at zero of Core/src/voxels.cpp:187.
+ * sino: (n_angles, n_h, n_v) log data; volume: nx*ny*nz floats (written);
+ * norms: NULL or niter doubles (|A^T r| per CGLS-family iteration).  The
+ * call uploads, solves on the current device and downloads; it blocks. */
+int ccpi_reconstruct(const ccpi_geometry *geometry, int alg, const float *sino, int niter,
+                     double regularize, double *norms, float *volume);
+
 /* ---------------------------------------------------------------------
  * Device-level calls (device buffers; asynchronous on `stream` unless
  * stated).  Replace the core projector and solver entry points the
@@ -316,8 +327,9 @@ void ccpi_session_destroy(ccpi_session *session);
  * it before any stream capture begins.  Iterations are host-driven (the
  * CCPI_SOLVE_PLAIN schedule).  All calls on one device share the scratch,
  * so calls that overlap in time (several host threads) race; each call
- * blocks until done, so sequential calls are safe.  Arguments and results
- * are as for ccpi_solve. */
+ * blocks until done, so sequential calls are safe.  The plan's device must
+ * be the current device (an error otherwise).  Arguments and results are as
+ * for ccpi_solve. */
 int ccpi_solve_noalloc(const ccpi_plan *plan, int alg, const float *d_sino,
                        float *d_x, int niterations, double regularize,
                        double *h_norms, void *stream);

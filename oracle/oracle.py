@@ -336,9 +336,7 @@ def ref_pb_reconstruct(alg, pixels, angles_deg, cor, ppv, niter, is_log, lam=0.0
     # cgls_regularize::reconstruct updates r_vox (a volume) with sinogram
     # extents (Core/src/Algorithms/cgls.cpp:386): pad every allocation by
     # the overrun ratio so that those writes land in padding
-    n_vox = int(dims[0]) * int(dims[1]) * int(dims[2])
-    n_pix = na * nh * int(dims[3])
-    pad = max(0.0, n_pix / max(n_vox, 1) - 1.0) + 0.05 if alg in (3, 4) else 0.0
+    pad = _reg_pad(alg, na * nh * int(dims[3]), int(dims[0]) * int(dims[1]) * int(dims[2]))
     x0p = None
     if x0 is not None:
         x0 = np.ascontiguousarray(x0, np.float32)
@@ -395,17 +393,30 @@ def ref_cb_geometry(na, nh, nv, ppv, s2s, s2d, px_h, px_v, mask_radius, pixels=N
     return dims, geom
 
 
+def _reg_pad(alg, n_pix, n_vox):
+    """Padding factor for the reference's allocations in its regularised
+    CGLS: cgls_regularize::reconstruct updates r_vox (a volume) with
+    sinogram extents (Core/src/Algorithms/cgls.cpp:386), so every allocation
+    is padded by the overrun ratio and those writes land in padding."""
+    return max(0.0, n_pix / max(n_vox, 1) - 1.0) + 0.05 if alg in (3, 4) else 0.0
+
+
 def ref_cb_reconstruct(alg, pixels, angles_deg, ppv, s2s, s2d, px_h, px_v, mask_radius, niter,
                        is_log, lam=0.0, nthreads=1):
     pixels = np.ascontiguousarray(pixels, np.float32)
     na, nh, nv = pixels.shape
     dims, _ = ref_cb_geometry(na, nh, nv, ppv, s2s, s2d, px_h, px_v, mask_radius)
     out = np.zeros(tuple(dims[:3]), np.float32)
-    rc = reference().ref_cb_reconstruct(alg, pixels, na, nh, nv,
-                                        np.ascontiguousarray(angles_deg, np.float32), ppv,
-                                        float(s2s), float(s2d), float(px_h), float(px_v),
-                                        float(mask_radius), niter, nthreads, int(bool(is_log)),
-                                        float(lam), out)
+    reference().ref_set_pad_factor(
+        _reg_pad(alg, na * nh * int(dims[3]), int(dims[0]) * int(dims[1]) * int(dims[2])))
+    try:
+        rc = reference().ref_cb_reconstruct(alg, pixels, na, nh, nv,
+                                            np.ascontiguousarray(angles_deg, np.float32), ppv,
+                                            float(s2s), float(s2d), float(px_h), float(px_v),
+                                            float(mask_radius), niter, nthreads,
+                                            int(bool(is_log)), float(lam), out)
+    finally:
+        reference().ref_set_pad_factor(0.0)
     if rc:
         raise RuntimeError(f"reference cone reconstruct failed ({rc})")
     return out
@@ -415,10 +426,15 @@ def ref_cb_solve_explicit(geom: Geometry, alg, sino, niter, lam=0.0, nthreads=1)
     lib = reference()
     a, h, v = (np.ascontiguousarray(x, np.float64) for x in (geom.angles, geom.h_pixels, geom.v_pixels))
     out = np.zeros(geom.shape, np.float32)
-    rc = lib.ref_cb_solve_explicit(alg, *geom.source, geom.detector_x, h, len(h), v, len(v), a,
-                                   len(a), np.ascontiguousarray(sino, np.float32),
-                                   np.array(geom.origin, np.float64), np.array(geom.size, np.float64),
-                                   *geom.shape, niter, float(lam), nthreads, out)
+    lib.ref_set_pad_factor(_reg_pad(alg, len(a) * len(h) * len(v), int(np.prod(geom.shape))))
+    try:
+        rc = lib.ref_cb_solve_explicit(alg, *geom.source, geom.detector_x, h, len(h), v, len(v),
+                                       a, len(a), np.ascontiguousarray(sino, np.float32),
+                                       np.array(geom.origin, np.float64),
+                                       np.array(geom.size, np.float64), *geom.shape, niter,
+                                       float(lam), nthreads, out)
+    finally:
+        lib.ref_set_pad_factor(0.0)
     if rc:
         raise RuntimeError(f"reference explicit cone solve failed ({rc})")
     return out

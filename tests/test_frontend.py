@@ -92,6 +92,30 @@ def test_setup_geometry_dicts():
     assert d["n_h"] == 24 and d["n_v"] == 8 and d["output_volume_z"] == 7
 
 
+@pytest.mark.parametrize("vshape,na,ppv", [((24, 20, 7), 16, 1), ((31, 40, 13), 9, 2),
+                                           ((64, 64, 16), 180, 1)])
+def test_setup_geometry_dicts_match_reference(vshape, na, ppv):
+    """pb_setup_geometry_from_image / _from_acquisition
+    (diamond_wrapper.cpp:559-631, :760-823) give the reference's numbers:
+    its padded row count and, from a sinogram, its reconstruction grid."""
+    import oracle as O
+    if not O.reference_available():
+        pytest.skip("oracle/_ref/libccpi_ref.so not built")
+    from ccpi.reconstruction.parallelbeam import alg
+    vx, vy, vz = vshape
+    width = max(vx, vy)
+    d = alg.pb_setup_geometry_from_image(np.zeros(vshape, np.float32), np.zeros(na), ppv)
+    dims, _ = O.ref_pb_geometry(na, vz, width, width / 2.0, ppv)
+    assert d == {"n_angles": na, "n_h": width, "n_v": int(dims[3]), "output_volume_x": vx,
+                 "output_volume_y": vy, "output_volume_z": vz}
+    nv, nh, cor = vz + 3, width + 5, width / 2.0 + 1.25
+    d = alg.pb_setup_geometry_from_acquisition(np.zeros((na, nv, nh), np.float32), np.zeros(na),
+                                               cor, ppv)
+    dims, _ = O.ref_pb_geometry(na, nv, nh, cor, ppv)
+    assert d == {"n_angles": na, "n_h": nh, "n_v": int(dims[3]), "output_volume_x": int(dims[0]),
+                 "output_volume_y": int(dims[1]), "output_volume_z": int(dims[2])}
+
+
 @pytest.mark.parametrize("na,nv,nh,cor,ppv", [(30, 7, 40, 0.0, 1), (45, 16, 64, 33.25, 2),
                                               (12, 5, 33, 16.0, 1)])
 def test_pb_geometry_matches_oracle_front_end(na, nv, nh, cor, ppv):
