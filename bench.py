@@ -46,7 +46,7 @@ CN, CNA, CND, CPIX, CS2O, CO2D = 512, 720, 768, 0.8, 500.0, 500.0
 CONE_WORKLOAD = ("cone-beam CGLS, 512^3 ellipsoid phantom (40), 720 angles over 2 pi, "
                  "768x768 detector at 0.8 mm, source/detector 500 mm, Poisson 5e3, explicit "
                  "512^3 grid of 1 mm voxels")
-CONE_SAMPLE_ANGLES = 32  # angle sample of the CPU baseline (a multiple of 16 host cores)
+CONE_SAMPLE_ANGLES = 48  # angle sample of the CPU baselines: divides 720, a multiple of 16 cores
 # parallel-beam SIRT/MLEM workload
 NA, NV, NH = 720, 256, 768
 PHANTOM = (512, 512, 256)
@@ -344,7 +344,7 @@ def run_reference(args):
     t_iter = max(tk - t0, 1e-9) / args.steps * (CNA / CONE_SAMPLE_ANGLES)
     v = 1.0 / t_iter
     cb = {"value": v, "unit": "iter/s", "cores": threads, "kind": "reference",
-          "sample": f"reference cone CGLS on {CONE_SAMPLE_ANGLES} of 720 angles, full 512^3 grid "
+          "sample": f"reference cone CGLS on {CONE_SAMPLE_ANGLES} of 720 angles (every {CNA // CONE_SAMPLE_ANGLES}th), full 512^3 grid "
                     f"and 768^2 detector; (t({args.steps} iterations) - t(0)) / {args.steps} "
                     f"scaled x{CNA // CONE_SAMPLE_ANGLES}"}
     print(json.dumps({
@@ -366,7 +366,7 @@ def sirt_cpu_baseline(sino_np_log):
     O = oracle()
     if not O.reference_available():
         return None
-    n = 32
+    n = CONE_SAMPLE_ANGLES
     idx = np.arange(0, NA, NA // n)[:n]
     ang = np.linspace(0.0, 180.0, NA, endpoint=False).astype(np.float32)[idx]
     pix = np.ascontiguousarray(np.transpose(sino_np_log[idx], (0, 2, 1)))

@@ -92,6 +92,12 @@ def _load():
     lib.ccpi_session_finish.argtypes = [_vp, _vp]
     lib.ccpi_session_destroy.argtypes = [_vp]
     lib.ccpi_session_destroy.restype = None
+    lib.ccpi_shard_create.argtypes = [_vp, _c_int, _vp, _vp, _c_dbl, _c_int, _vp, _vp, _vp,
+                                      _vp, _vp, P(_vp)]
+    lib.ccpi_shard_stage.argtypes = [_vp, _c_int]
+    lib.ccpi_shard_finish.argtypes = [_vp, _vp]
+    lib.ccpi_shard_destroy.argtypes = [_vp]
+    lib.ccpi_shard_destroy.restype = None
     return lib
 
 

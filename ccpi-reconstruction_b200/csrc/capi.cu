@@ -958,4 +958,44 @@ void ccpi_session_destroy(ccpi_session *session) {
     ccpi::session_destroy(session);
 }
 
+int ccpi_shard_create(const ccpi_plan *plan, int alg, const float *d_sino, float *d_x,
+                      double regularize, int max_iterations, double *d_sum, float *d_edges,
+                      const float *d_halo_lo, const float *d_halo_hi, void *stream,
+                      ccpi_shard **shard) {
+  ccpi::g_last_error.clear();
+  if (!plan || !d_sino || !d_x || !shard) {
+    set_error("ccpi_shard_create: null argument");
+    return 1;
+  }
+  int rc = 0;
+  *shard = static_cast<ccpi_shard *>(ccpi::shard_create(plan, alg, d_sino, d_x, regularize,
+                                                         max_iterations, d_sum, d_edges,
+                                                         d_halo_lo, d_halo_hi,
+                                                         cudaStream_t(stream), &rc));
+  return rc;
+}
+
+int ccpi_shard_stage(ccpi_shard *shard, int stage) {
+  ccpi::g_last_error.clear();
+  if (!shard) {
+    set_error("ccpi_shard_stage: null shard");
+    return 1;
+  }
+  return ccpi::shard_stage(shard, stage);
+}
+
+int ccpi_shard_finish(ccpi_shard *shard, double *h_norms) {
+  ccpi::g_last_error.clear();
+  if (!shard) {
+    set_error("ccpi_shard_finish: null shard");
+    return 1;
+  }
+  return ccpi::shard_finish(shard, h_norms);
+}
+
+void ccpi_shard_destroy(ccpi_shard *shard) {
+  if (shard)
+    ccpi::shard_destroy(shard);
+}
+
 } // extern "C"

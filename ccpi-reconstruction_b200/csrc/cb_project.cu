@@ -21,6 +21,8 @@
 // taller than 1024 voxels use cb_bp_kernel, whose warps spread rows into a
 // shared-memory accumulator with float atomics (unspecified order, equal to
 // the reference to float rounding).
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -414,8 +416,11 @@ __global__ void __launch_bounds__(kFpWarps * 32)
       for (int q = 0; q < RPL; q++) {
         const int v = vb + q * 32 + lane;
         if (v < g.nv) {
-          const float val = __fmul_rn(acc[q], g.dconv[i64(h) * g.nv + v]);
-          pix[rbase + v] = cb_fp_epi<EPI>(val, rbase + v, e, ssq);
+          const float dcv = g.dconv[i64(h) * g.nv + v];
+          const float out = cb_fp_epi<EPI>(__fmul_rn(acc[q], dcv), rbase + v, e, ssq);
+          // the SIRT / MLEM residual is the back projector's input: with
+          // e.pre it is stored times d_conv (the reference's dpixels)
+          pix[rbase + v] = ((EPI == EPI_SIRT || EPI == EPI_MLEM) && e.pre) ? __fmul_rn(out, dcv) : out;
         }
       }
     }
@@ -633,7 +638,10 @@ constexpr int kGaThreads = 256;
 constexpr int kGaChunk = 64;
 constexpr int kGaRays = kBpMaxRaysPerAngle; // slots per angle
 #ifndef CB_GA_STAGE
-#define CB_GA_STAGE 3
+#define CB_GA_STAGE 3 // rays per stage when the kernel multiplies by d_conv itself
+#endif
+#ifndef CB_GA_STAGE_PRE
+#define CB_GA_STAGE_PRE 4 // rays per stage on a sinogram already scaled by d_conv
 #endif
 #ifndef CB_GA_FAST
 #define CB_GA_FAST 1
@@ -641,14 +649,18 @@ constexpr int kGaRays = kBpMaxRaysPerAngle; // slots per angle
 #ifndef CB_GA_PACKED
 #define CB_GA_PACKED 1
 #endif
-constexpr int kGaStage = CB_GA_STAGE;
+#ifndef CB_GA_TILE
+#define CB_GA_TILE 16 // CTAs walk the columns in 16 x 16 tiles (0: row-major order)
+#endif
+constexpr int kGaStageMax = 8;
 
 __host__ __device__ inline int round4(int n) { return (n + 3) & ~3; }
 
-// Shared-memory layout of cb_bp_gather (offsets in 4-byte words).
+// Shared-memory layout of cb_bp_gather (offsets in 4-byte words) for
+// `st` rays per stage.
 struct GaLayout {
   int vz, dz, iz, seg_h, seg_a0, seg_a1, cnt, off, map, fr, prow, drow, total;
-  __host__ __device__ GaLayout(int nz, int nv) {
+  __host__ __device__ GaLayout(int nz, int nv, int st) {
     vz = 0;
     dz = vz + cb_vz_floats(nz);
     iz = dz + round4(nv);
@@ -659,14 +671,33 @@ struct GaLayout {
     off = cnt + round4(kGaChunk + 1);
     map = off + round4(kGaChunk + 1);
     fr = map + kGaChunk * kGaRays;
-    prow = fr + kGaStage * round4(nz + 2);
-    drow = prow + kGaStage * round4(nv);
-    total = drow + kGaStage * round4(nv);
+    prow = fr + st * round4(nz + 2);
+    drow = prow + st * round4(nv);
+    total = drow + st * round4(nv);
   }
 };
 
+// Voxel column of CTA b: CTAs run through the xy plane in T x T tiles, so
+// the columns in flight at any time form a compact patch whose rays (and
+// the sinogram rows they read) overlap and stay in L2.  Any order gives the
+// same sums: each CTA owns its column.
+__device__ __forceinline__ int cb_ga_column(int b, int nx, int ny) {
+#if CB_GA_TILE > 0
+  constexpr int T = CB_GA_TILE;
+  if (nx % T != 0 || ny % T != 0)
+    return b;
+  const int tile = b / (T * T), in = b - tile * (T * T);
+  const int tpr = ny / T; // tiles along y
+  const int ti = tile / tpr, tj = tile - ti * tpr;
+  return (ti * T + in / T) * ny + tj * T + in % T;
+#else
+  return b;
+#endif
+}
+
 // Stage the rays of angles [ac, ac + nac) in list order: slots per angle,
-// then a prefix over angles and a flat map.  Returns the ray count.
+// then a prefix over angles and a flat map.  Returns the ray count.  Each
+// slot holds the ray's detector column h and its entry and exit alphas.
 __device__ int cb_ga_stage_rays(const Geom &g, int ac, int nac, double x0, double xn, double y0,
                                 double yn, int *seg_h, float *seg_a0, float *seg_a1, int *cnt,
                                 int *off, int *map, int *ovf) {
@@ -720,14 +751,18 @@ __device__ __forceinline__ void cb_ga_mark(int *f, int kp, int k, int v, int nz)
 
 // Register bound: 4 CTAs per SM for one voxel per thread; taller columns
 // need more shared memory per CTA, which allows 3 (or 2) anyway.
-template <int EPI, int NZT, int RMAX>
+// PRE: the sinogram is already scaled by d_conv (the reference's dpixels,
+// c2D.cpp:1096-1117, formed by the producer of the back projector's input),
+// so a staged row is one load and no multiply.  ST rays per stage.
+template <int EPI, int NZT, int RMAX, bool PRE, int ST>
 __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
     cb_bp_gather(Geom g, const float *__restrict__ pix, float *__restrict__ vol, Epi e,
                  int *err) {
+  static_assert(ST <= kGaStageMax, "stage too large");
   extern __shared__ unsigned char smem_raw[];
   int *W = reinterpret_cast<int *>(smem_raw);
   const int nz = g.nz, nv = g.nv, nzm1 = nz - 1, mid = g.mid;
-  const GaLayout L(nz, nv);
+  const GaLayout L(nz, nv, ST);
   float *svz = reinterpret_cast<float *>(W + L.vz);
   float *sdz = reinterpret_cast<float *>(W + L.dz);
   float *siz = reinterpret_cast<float *>(W + L.iz);
@@ -739,12 +774,12 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
   float *drow = reinterpret_cast<float *>(W + L.drow); // their d_conv rows
   const int frs = round4(nz + 2), prs = round4(nv);
   __shared__ int s_minv, s_maxv, s_ovf;
-  __shared__ int s_kf[kGaStage], s_kl[kGaStage]; // slices of a staged ray's first/last band row
+  __shared__ int s_kf[ST], s_kl[ST]; // slices of a staged ray's first/last band row
   // the column's square; kept in shared memory so that its FP64 corners
   // hold no registers through the row and voxel phases
   __shared__ double s_box[4];
   const int tid = threadIdx.x;
-  const int col = blockIdx.x;
+  const int col = cb_ga_column(blockIdx.x, g.nx, g.ny);
   const int i = col / g.ny, j = col - (col / g.ny) * g.ny;
   for (int t = tid; t <= nz; t += blockDim.x)
     svz[t] = g.vz[t];
@@ -801,23 +836,30 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
     const int nac = min(kGaChunk, g.na - ac);
     const int nseg = cb_ga_stage_rays(g, ac, nac, s_box[0], s_box[1], s_box[2], s_box[3], seg_h,
                                       seg_a0, seg_a1, cnt, off, map, &s_ovf);
-    for (int s0 = 0; s0 < nseg; s0 += kGaStage) {
-      const int ns = min(kGaStage, nseg - s0);
+    for (int s0 = 0; s0 < nseg; s0 += ST) {
+      const int ns = min(ST, nseg - s0);
       // 1) this thread's band rows v = min_v + tid + r * 256 of every staged
-      //    ray: pixel and d_conv values, all loads issued together
-      float pv[kGaStage][RMAX], dv[kGaStage][RMAX];
+      //    ray: pixel values (times d_conv unless pre-scaled), all loads
+      //    issued together
+      float pv[ST][RMAX], dv[PRE ? 1 : ST][RMAX];
 #pragma unroll
-      for (int s = 0; s < kGaStage; s++) {
+      for (int s = 0; s < ST; s++) {
         const int m = map[s0 + (s < ns ? s : 0)];
-        const int a = ac + m / kGaRays, h = seg_h[m];
-        const float *prw = pix + (i64(a) * g.nh + h) * nv;
-        const float *drw = g.dconv + i64(h) * nv;
+        const int h = seg_h[m];
+        const float *prw = pix + (i64(ac + m / kGaRays) * g.nh + h) * nv;
 #pragma unroll
         for (int r = 0; r < RMAX; r++) {
           const int v = min_v + tid + r * kGaThreads;
           const bool ok = s < ns && v < max_v;
           pv[s][r] = ok ? __ldg(prw + v) : 0.0f;
-          dv[s][r] = ok ? __ldg(drw + v) : 0.0f;
+        }
+        if (!PRE) {
+          const float *drw = g.dconv + i64(h) * nv;
+#pragma unroll
+          for (int r = 0; r < RMAX; r++) {
+            const int v = min_v + tid + r * kGaThreads;
+            dv[PRE ? 0 : s][r] = (s < ns && v < max_v) ? __ldg(drw + v) : 0.0f;
+          }
         }
       }
       // 2) per ray: the first band row of every slice index (the whole
@@ -826,7 +868,7 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
       //    them (c2D.cpp:694-711): c1 = p (mz - a0) goes to slice k, c2 =
       //    p (a1 - mz) to k - 1 below the source row, to k + 1 from it on
 #pragma unroll
-      for (int s = 0; s < kGaStage; s++) {
+      for (int s = 0; s < ST; s++) {
         if (s >= ns)
           break;
         const int m = map[s0 + s];
@@ -880,8 +922,9 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
             const float2 pl =
                 mul2_rn(make_float2(svz[kz0], svz[kz1]), make_float2(rsi[r], rsi[r + 1]));
             const float2 mz = make_float2(fmin_ref(pl.x, a1), fmin_ref(pl.y, a1));
-            const float2 p = mul2_rn(make_float2(pv[s][r], pv[s][r + 1]),
-                                     make_float2(dv[s][r], dv[s][r + 1]));
+            const float2 p = PRE ? make_float2(pv[s][r], pv[s][r + 1])
+                                 : mul2_rn(make_float2(pv[s][r], pv[s][r + 1]),
+                                           make_float2(dv[PRE ? 0 : s][r], dv[PRE ? 0 : s][r + 1]));
             const float2 w1 = mul2_rn(p, sub2_rn(mz, a02)), w2 = mul2_rn(p, sub2_rn(a12, mz));
             if (v0 < max_v) {
               c1[v0] = w1.x;
@@ -903,7 +946,7 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
               cb_ga_mark(f, int(__fadd_rn(pzbz, __fmul_rn(av, rsp[r]))), k, v, nz);
             const int kz = min(max(v < mid ? k : k + 1, 0), nz);
             const float mz = fmin_ref(__fmul_rn(svz[kz], rsi[r]), a1);
-            const float p = __fmul_rn(pv[s][r], dv[s][r]);
+            const float p = PRE ? pv[s][r] : __fmul_rn(pv[s][r], dv[PRE ? 0 : s][r]);
             c1[v] = __fmul_rn(p, __fsub_rn(mz, a0));
             c2[v] = __fmul_rn(p, __fsub_rn(a1, mz));
           }
@@ -951,10 +994,10 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
                                         seg_h, seg_a0, seg_a1, cnt, off, map, &s_ovf);
       for (int s = 0; s < nseg; s++) {
         const int m = map[s];
-        const int a = ac + m / kGaRays, h = seg_h[m];
+        const int h = seg_h[m];
         const float a0 = seg_a0[m], a1 = seg_a1[m];
         const float av = __fmul_rn(a0, inv_dz);
-        const float *prw = pix + (i64(a) * g.nh + h) * nv;
+        const float *prw = pix + (i64(ac + m / kGaRays) * g.nh + h) * nv;
         const float *drw = g.dconv + i64(h) * nv;
 #pragma unroll
         for (int q = 0; q < NZT; q++) {
@@ -967,7 +1010,7 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
               break; // k only falls as v falls (and k < 0 ends the reference's loop)
             if (k > K + 1)
               continue;
-            const float p = __fmul_rn(__ldg(prw + v), __ldg(drw + v));
+            const float p = PRE ? __ldg(prw + v) : __fmul_rn(__ldg(prw + v), __ldg(drw + v));
             if (k > 0) {
               const float mz = fmin_ref(__fmul_rn(svz[k], siz[v]), a1);
               acc[q] = __fadd_rn(acc[q], __fmul_rn(p, k == K ? __fsub_rn(mz, a0)
@@ -983,7 +1026,7 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
               break; // k only rises with v (and k > nz - 1 ends the reference's loop)
             if (k < K - 1)
               continue;
-            const float p = __fmul_rn(__ldg(prw + v), __ldg(drw + v));
+            const float p = PRE ? __ldg(prw + v) : __fmul_rn(__ldg(prw + v), __ldg(drw + v));
             const float mz = fmin_ref(__fmul_rn(svz[k + 1], siz[v]), a1);
             if (k == K)
               acc[q] = __fadd_rn(acc[q], __fmul_rn(p, __fsub_rn(mz, a0)));
@@ -1076,7 +1119,10 @@ size_t cb_bp_atomic_smem(const Geom &g) {
   return size_t(g.nz) * sizeof(float) +
          size_t(kBpAngleChunk) * kBpMaxRaysPerAngle * (sizeof(int) + 2 * sizeof(float));
 }
-size_t cb_bp_gather_smem(const Geom &g) { return size_t(GaLayout(g.nz, g.nv).total) * 4; }
+// the larger of the two stage sizes' layouts
+size_t cb_bp_gather_smem(const Geom &g) {
+  return size_t(GaLayout(g.nz, g.nv, std::max(CB_GA_STAGE, CB_GA_STAGE_PRE)).total) * 4;
+}
 // voxels per thread of the deterministic gather, 0 if it does not apply
 int cb_bp_gather_nzt(const Geom &g) {
   if (cb_bp_gather_smem(g) > 200 * 1024 || g.nv > 4 * kGaThreads)
@@ -1111,8 +1157,14 @@ int cb_prepare(const Geom &g) {
       e2 = cudaErrorInvalidValue;
   if (cb_bp_gather_nzt(g)) {
 #define CB_GA_EPI(Z, R)                                                                    \
-  (const void *)cb_bp_gather<EPI_STORE, Z, R>, (const void *)cb_bp_gather<EPI_NORM, Z, R>,  \
-      (const void *)cb_bp_gather<EPI_SIRT, Z, R>, (const void *)cb_bp_gather<EPI_MLEM, Z, R>
+  (const void *)cb_bp_gather<EPI_STORE, Z, R, false, CB_GA_STAGE>,                          \
+      (const void *)cb_bp_gather<EPI_NORM, Z, R, false, CB_GA_STAGE>,                       \
+      (const void *)cb_bp_gather<EPI_SIRT, Z, R, false, CB_GA_STAGE>,                       \
+      (const void *)cb_bp_gather<EPI_MLEM, Z, R, false, CB_GA_STAGE>,                       \
+      (const void *)cb_bp_gather<EPI_STORE, Z, R, true, CB_GA_STAGE_PRE>,                   \
+      (const void *)cb_bp_gather<EPI_NORM, Z, R, true, CB_GA_STAGE_PRE>,                    \
+      (const void *)cb_bp_gather<EPI_SIRT, Z, R, true, CB_GA_STAGE_PRE>,                    \
+      (const void *)cb_bp_gather<EPI_MLEM, Z, R, true, CB_GA_STAGE_PRE>
 #define CB_GA_ALL(Z) CB_GA_EPI(Z, 1), CB_GA_EPI(Z, 2), CB_GA_EPI(Z, 3), CB_GA_EPI(Z, 4)
     const void *gas[] = {CB_GA_ALL(1), CB_GA_ALL(2), CB_GA_ALL(4)};
 #undef CB_GA_EPI
@@ -1146,33 +1198,65 @@ int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi 
 }
 
 namespace {
+// out[a][h][v] = in[a][h][v] * d_conv[h][v]: the reference's dpixels
+// (c2D.cpp:1096-1117), the same float products the back projector would
+// form row by row.
+__global__ void cb_prescale_kernel(const float *__restrict__ in, float *__restrict__ out,
+                                   const float *__restrict__ dconv, i64 per_angle, i64 n) {
+  for (i64 i = blockIdx.x * i64(blockDim.x) + threadIdx.x; i < n;
+       i += i64(gridDim.x) * blockDim.x)
+    out[i] = __fmul_rn(in[i], dconv[i % per_angle]);
+}
+
+template <int EPI, bool PRE, int ST>
+void launch_cb_ga(const Geom &g, int nzt, int rmax, const float *pix, float *vol, const Epi &e,
+                  int *err, cudaStream_t st) {
+  const int ncol = g.nx * g.ny;
+  const size_t gsm = cb_bp_gather_smem(g);
+#define CB_GA_GO(Z)                                                                        \
+  (rmax == 1   ? cb_bp_gather<EPI, Z, 1, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err) \
+   : rmax == 2 ? cb_bp_gather<EPI, Z, 2, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err) \
+   : rmax == 3 ? cb_bp_gather<EPI, Z, 3, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err) \
+               : cb_bp_gather<EPI, Z, 4, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err))
+  if (nzt == 1)
+    CB_GA_GO(1);
+  else if (nzt == 2)
+    CB_GA_GO(2);
+  else
+    CB_GA_GO(4);
+#undef CB_GA_GO
+}
+
 template <int EPI>
 void launch_cb_bp(const Geom &g, const float *pix, float *vol, const Epi &e, int *err,
                   cudaStream_t st) {
   const int ncol = g.nx * g.ny;
-  const size_t gsm = cb_bp_gather_smem(g);
-  const int rmax = cb_bp_gather_rmax(g);
-#define CB_GA_GO(Z)                                                                        \
-  (rmax == 1   ? cb_bp_gather<EPI, Z, 1><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err)  \
-   : rmax == 2 ? cb_bp_gather<EPI, Z, 2><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err)  \
-   : rmax == 3 ? cb_bp_gather<EPI, Z, 3><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err)  \
-               : cb_bp_gather<EPI, Z, 4><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err))
-  switch (cb_bp_gather_nzt(g)) {
+  const int nzt = cb_bp_gather_nzt(g), rmax = cb_bp_gather_rmax(g);
+  if (nzt && e.pre) {
+    launch_cb_ga<EPI, true, CB_GA_STAGE_PRE>(g, nzt, rmax, pix, vol, e, err, st);
+    return;
+  }
+  switch (nzt) {
   case 1:
-    CB_GA_GO(1);
-    break;
   case 2:
-    CB_GA_GO(2);
-    break;
   case 4:
-    CB_GA_GO(4);
+    launch_cb_ga<EPI, false, CB_GA_STAGE>(g, nzt, rmax, pix, vol, e, err, st);
     break;
   default:
     cb_bp_kernel<EPI><<<ncol, kBpThreads, cb_bp_atomic_smem(g), st>>>(g, pix, vol, e, err);
   }
-#undef CB_GA_GO
 }
 } // namespace
+
+bool cb_bp_takes_prescaled(const Geom &g) {
+  return cb_bp_gather_nzt(g) != 0 && i64(g.na) * g.nh < (i64(1) << 31);
+}
+
+void cb_prescale(const Geom &g, const float *in, float *out, cudaStream_t st) {
+  const i64 per = i64(g.nh) * g.nv, n = i64(g.na) * per;
+  const i64 blocks = std::min<i64>((n + 255) / 256, i64(sm_count()) * 8);
+  cb_prescale_kernel<<<int(std::max<i64>(blocks, 1)), 256, 0, st>>>(in, out, g.dconv, per, n);
+}
 
 int cb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
                 int *err, cudaStream_t st) {

@@ -61,6 +61,9 @@ struct Epi {
   const float *w;    // per-element weight: R (SIRT fp), C (SIRT bp), N (MLEM bp)
   float *x;          // volume updated in place by the back-projector epilogues
   double *partials;  // one FP64 partial sum of squares per CTA (NORM modes)
+  int pre;           // cone beam: the back projector's input is already scaled by
+                     // d_conv, and the forward projector's SIRT / MLEM output is
+                     // stored scaled (the reference's dpixels, c2D.cpp:1096-1117)
 };
 
 enum EpiMode {

@@ -387,11 +387,26 @@ size_t layout(const ccpi_plan *p, int alg, int niter, char *base, Work *w) {
   return off;
 }
 
+// The back projection of the CGLS residual r.  Cone beam: the residual is
+// first scaled by d_conv into q (free once r is updated), the reference's
+// dpixels, and the back projector reads the scaled copy.
+int backward_residual(const ccpi_plan *p, const Work &W, Epi e, cudaStream_t st) {
+  if (p->g.kind == CCPI_CONE && cb_bp_takes_prescaled(p->g)) {
+    cb_prescale(p->g, W.r, W.q, st);
+    e.pre = 1;
+    return backward(p, W.q, W.s, EPI_NORM, e, st);
+  }
+  return backward(p, W.r, W.s, EPI_NORM, e, st);
+}
+
 // One iteration of `alg` (kernels only; capturable).
 int iterate(const ccpi_plan *p, int alg, const float *sino, float *x, const Work &W,
             float lambda, cudaStream_t st) {
   const i64 V = p->nvox, P = p->npix;
   Epi e{};
+  // cone SIRT / MLEM: the forward projector stores its residual scaled by
+  // d_conv, which the back projector then reads as is
+  const int pre = (p->g.kind == CCPI_CONE && cb_bp_takes_prescaled(p->g)) ? 1 : 0;
   int rc = 0;
   switch (alg) {
   case CCPI_CGLS:
@@ -400,13 +415,14 @@ int iterate(const ccpi_plan *p, int alg, const float *sino, float *x, const Work
     k_cgls_scalars(S_ALPHA, W.part1, p->fp_grid, nullptr, 0, W.scal, nullptr, st);
     k_axpy_scalar(W.r, W.q, P, W.scal, 1, -1.0f, st);
     e.partials = W.part2;
-    rc |= backward(p, W.r, W.s, EPI_NORM, e, st);
+    rc |= backward_residual(p, W, e, st);
     k_cgls_scalars(S_BETA, W.part2, p->bp_parts, nullptr, 0, W.scal, W.norms, st);
     k_cgls_xd(x, W.d, W.s, V, W.scal, st);
     break;
   case CCPI_SIRT:
     e.b = sino;
     e.w = W.q; // R
+    e.pre = pre;
     rc |= forward(p, x, W.r, EPI_SIRT, e, st);
     e.w = W.d; // C
     e.x = x;
@@ -414,6 +430,7 @@ int iterate(const ccpi_plan *p, int alg, const float *sino, float *x, const Work
     break;
   case CCPI_MLEM:
     e.b = sino;
+    e.pre = pre;
     rc |= forward(p, x, W.r, EPI_MLEM, e, st);
     e.w = W.d; // N
     e.x = x;
@@ -431,7 +448,7 @@ int iterate(const ccpi_plan *p, int alg, const float *sino, float *x, const Work
     k_add_scaled(W.u, x, W.d, V, W.scal, st);
     k_reg_step(alg, W.u, x, p->g.nx, p->g.ny, p->g.nz, lambda, st);
     e.partials = W.part2;
-    rc |= backward(p, W.r, W.s, EPI_NORM, e, st);
+    rc |= backward_residual(p, W, e, st);
     k_cgls_scalars(S_BETA, W.part2, p->bp_parts, nullptr, 0, W.scal, W.norms, st);
     k_cgls_d(W.d, W.s, V, W.scal, st);
     break;
@@ -646,6 +663,176 @@ int session_finish(void *h, double *h_norms) {
 }
 
 void session_destroy(void *h) { delete static_cast<Session *>(h); }
+
+// ---- z-sharded CGLS family: one slab of a parallel-beam volume per rank
+//
+// A parallel-beam volume cut along z into slabs (rows map to their own
+// slices, so each rank projects its slab alone; the reference's MPI split,
+// voxels.cpp:27-45) needs, per CGLS iteration, the two step-scalar sums over
+// all ranks and, for TV, the z planes next to each cut.  The iteration of
+// iterate() is split at those points into stages; between stages the caller
+// all-reduces one double (sum) and, for TV, swaps edge planes into the
+// neighbours' halo buffers.  With one rank and no halos the stages give the
+// unsharded solve bit for bit.
+struct Shard {
+  const ccpi_plan *plan = nullptr;
+  int alg = 0;
+  const float *sino = nullptr;
+  float *x = nullptr;
+  float lambda = 0.0f;
+  int max_iter = 0, done = 0;
+  int next = SHARD_SETUP; // the stage the protocol expects next
+  cudaStream_t st = nullptr;
+  void *ws = nullptr;
+  Work W;
+  double *sum = nullptr;              // caller-owned, 1 double
+  float *edge_lo = nullptr, *edge_hi = nullptr;   // caller-owned, nx * ny each
+  const float *halo_lo = nullptr, *halo_hi = nullptr; // caller-owned or NULL
+  ~Shard() {
+    if (ws)
+      cudaFree(ws);
+  }
+};
+
+void *shard_create(const ccpi_plan *p, int alg, const float *sino, float *x, double lambda,
+                   int max_iter, double *sum, float *edges, const float *halo_lo,
+                   const float *halo_hi, cudaStream_t st, int *rc) {
+  *rc = 0;
+  if (alg != CCPI_CGLS && alg != CCPI_CGLS_TIKHONOV && alg != CCPI_CGLS_TV) {
+    set_error("ccpi_shard_create: sharded solves are the CGLS family (SIRT and MLEM need no "
+              "exchange: solve each slab alone)");
+    *rc = 1;
+    return nullptr;
+  }
+  if (p->g.kind != CCPI_PARALLEL || max_iter < 0 || !sum || !edges) {
+    set_error("ccpi_shard_create: needs a parallel-beam plan, an iteration budget, a sum and "
+              "an edge buffer");
+    *rc = 1;
+    return nullptr;
+  }
+  Shard *S = new Shard();
+  S->plan = p;
+  S->alg = alg;
+  S->sino = sino;
+  S->x = x;
+  S->lambda = float(lambda);
+  S->max_iter = max_iter;
+  S->st = st;
+  S->sum = sum;
+  const i64 nxy = i64(p->g.nx) * p->g.ny;
+  S->edge_lo = edges;
+  S->edge_hi = edges + nxy;
+  S->halo_lo = halo_lo;
+  S->halo_hi = halo_hi;
+  const size_t need = layout(p, alg, max_iter, nullptr, nullptr);
+  if (!cuda_ok(cudaMalloc(&S->ws, need), "ccpi_shard_create: workspace")) {
+    delete S;
+    *rc = 2;
+    return nullptr;
+  }
+  layout(p, alg, max_iter, static_cast<char *>(S->ws), &S->W);
+  return S;
+}
+
+int shard_stage(void *h, int stage) {
+  Shard *S = static_cast<Shard *>(h);
+  if (stage != S->next) {
+    set_error("ccpi_shard_stage: stage " + std::to_string(stage) + " out of order (expected " +
+              std::to_string(S->next) + ")");
+    return 1;
+  }
+  if (stage == SHARD_FORWARD && S->done >= S->max_iter) {
+    set_error("ccpi_shard_stage: iteration budget of the shard exceeded");
+    return 1;
+  }
+  const ccpi_plan *p = S->plan;
+  const Work &W = S->W;
+  const cudaStream_t st = S->st;
+  const i64 V = p->nvox, P = p->npix;
+  const int nx = p->g.nx, ny = p->g.ny, nz = p->g.nz, nb = sumsq_blocks();
+  const bool reg = S->alg != CCPI_CGLS;
+  Epi e{};
+  int rc = 0;
+  switch (stage) {
+  case SHARD_SETUP:
+    // the residual starts at b (cgls.cpp:33-46); d = A^T r
+    cudaMemsetAsync(W.scal, 0, sizeof(double) * 8, st);
+    cudaMemcpyAsync(W.r, S->sino, size_t(P) * 4, cudaMemcpyDeviceToDevice, st);
+    e.partials = W.part2;
+    rc |= backward(p, W.r, W.d, EPI_NORM, e, st);
+    k_shard_scalars(SH_LOCAL, W.part2, p->bp_parts, nullptr, 0, S->sum, W.scal, nullptr, st);
+    if (reg)
+      cudaMemsetAsync(W.t, 0, size_t(V) * 4, st);
+    k_pack_edges(W.d, nx, ny, nz, S->edge_lo, S->edge_hi, st);
+    S->next = SHARD_FORWARD;
+    break;
+  case SHARD_FORWARD:
+    if (S->done == 0)
+      k_shard_scalars(SH_INIT, nullptr, 0, nullptr, 0, S->sum, W.scal, nullptr, st);
+    e.partials = W.part1;
+    rc |= forward(p, W.d, W.q, EPI_NORM, e, st);
+    if (reg)
+      k_reg_accumulate(S->alg, W.d, W.t, nx, ny, nz, S->lambda, W.part2, nb, st, S->halo_lo,
+                       S->halo_hi);
+    k_shard_scalars(SH_LOCAL, W.part1, p->fp_grid, reg ? W.part2 : nullptr, nb, S->sum, W.scal,
+                    nullptr, st);
+    S->next = SHARD_UPDATE;
+    break;
+  case SHARD_UPDATE:
+    k_shard_scalars(SH_ALPHA, nullptr, 0, nullptr, 0, S->sum, W.scal, nullptr, st);
+    k_axpy_scalar(W.r, W.q, P, W.scal, 1, -1.0f, st);
+    if (reg) {
+      k_add_scaled(W.u, S->x, W.d, V, W.scal, st);
+      k_pack_edges(W.u, nx, ny, nz, S->edge_lo, S->edge_hi, st);
+    }
+    S->next = SHARD_BACKWARD;
+    break;
+  case SHARD_BACKWARD:
+    if (reg)
+      k_reg_step(S->alg, W.u, S->x, nx, ny, nz, S->lambda, st, S->halo_lo, S->halo_hi);
+    e.partials = W.part2;
+    rc |= backward(p, W.r, W.s, EPI_NORM, e, st);
+    k_shard_scalars(SH_LOCAL, W.part2, p->bp_parts, nullptr, 0, S->sum, W.scal, nullptr, st);
+    S->next = SHARD_NEXT;
+    break;
+  case SHARD_NEXT:
+    k_shard_scalars(SH_BETA, nullptr, 0, nullptr, 0, S->sum, W.scal, W.norms, st);
+    if (reg) {
+      k_cgls_d(W.d, W.s, V, W.scal, st);
+      k_pack_edges(W.d, nx, ny, nz, S->edge_lo, S->edge_hi, st);
+    } else {
+      k_cgls_xd(S->x, W.d, W.s, V, W.scal, st);
+    }
+    S->done++;
+    S->next = SHARD_FORWARD;
+    break;
+  default:
+    set_error("ccpi_shard_stage: unknown stage");
+    return 1;
+  }
+  if (!cuda_ok(cudaGetLastError(), "ccpi_shard_stage: launch"))
+    rc |= 4;
+  return rc;
+}
+
+int shard_finish(void *h, double *h_norms) {
+  Shard *S = static_cast<Shard *>(h);
+  if (S->next != SHARD_FORWARD) {
+    set_error("ccpi_shard_finish: the last iteration is incomplete (finish after "
+              "CCPI_SHARD_NEXT or CCPI_SHARD_SETUP)");
+    return 1;
+  }
+  k_clamp0(S->x, S->plan->nvox, S->st);
+  if (!cuda_ok(cudaStreamSynchronize(S->st), "ccpi_shard_finish: execution"))
+    return 8;
+  if (!check_err(S->plan))
+    return 16;
+  if (h_norms && S->done > 0)
+    cudaMemcpy(h_norms, S->W.norms, sizeof(double) * S->done, cudaMemcpyDeviceToHost);
+  return 0;
+}
+
+void shard_destroy(void *h) { delete static_cast<Shard *>(h); }
 
 int solve(const ccpi_plan *p, int alg, const float *sino, float *x, int niter, double lambda,
           double *h_norms, int flags, void *ws, size_t ws_bytes, cudaStream_t st) {

@@ -46,6 +46,15 @@ int session_finish(void *s, double *h_norms);
 void session_destroy(void *s);
 int solve_batched(int n, const ccpi_plan *const *plans, int alg, const float *const *sino,
                   float *const *x, int niter, const double *lambda, cudaStream_t st);
+// z-sharded CGLS family (see engine.cu); stages as CCPI_SHARD_* in the C ABI
+enum ShardStage { SHARD_SETUP = 0, SHARD_FORWARD = 1, SHARD_UPDATE = 2, SHARD_BACKWARD = 3,
+                  SHARD_NEXT = 4 };
+void *shard_create(const ccpi_plan *p, int alg, const float *sino, float *x, double lambda,
+                   int max_iter, double *sum, float *edges, const float *halo_lo,
+                   const float *halo_hi, cudaStream_t st, int *rc);
+int shard_stage(void *s, int stage);
+int shard_finish(void *s, double *h_norms);
+void shard_destroy(void *s);
 // AML ring-artefact filter on a device sinogram [angle][h][v], in place
 // (aml.cu); synchronises st.
 int aml_ring_filter(float *d_sino, int na, int nh, int nv, double param_n, double param_r,

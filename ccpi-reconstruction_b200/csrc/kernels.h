@@ -20,6 +20,12 @@ int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi 
                const int2 *hrange, int grid, cudaStream_t st);
 int cb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
                 int *err, cudaStream_t st);
+// The cone back projector accepts a sinogram pre-scaled by d_conv (Epi::pre)
+// for this geometry; cb_prescale writes that scaled copy.
+bool cb_bp_takes_prescaled(const Geom &g);
+void cb_prescale(const Geom &g, const float *in, float *out, cudaStream_t st);
+// Streaming multiprocessors of the current device (engine.cu).
+int sm_count();
 
 // vector kernels (vec_ops.cu)
 void k_fill(float *p, i64 n, float v, cudaStream_t st);
@@ -44,13 +50,23 @@ void k_cgls_d(float *d, const float *sv, i64 n, const double *s, cudaStream_t st
 void k_add_scaled(float *out, const float *in, const float *d, i64 n, const double *s,
                   cudaStream_t st);
 
-// regularisers (vec_ops.cu).  alg 3 Tikhonov, 4 TV.
+// regularisers (vec_ops.cu).  alg 3 Tikhonov, 4 TV.  lo / hi (may be NULL):
+// the z planes just below and above a slab of a volume cut along z ([x][y]
+// each), read by the TV stencil in place of the mirrored neighbour.
 // acc += lambda * L(a), with per-CTA FP64 sum of squares of the new acc
 void k_reg_accumulate(int alg, const float *a, float *acc, int nx, int ny, int nz,
-                      float lambda, double *partials, int nblocks, cudaStream_t st);
+                      float lambda, double *partials, int nblocks, cudaStream_t st,
+                      const float *lo = nullptr, const float *hi = nullptr);
 // out = a + lambda * L(a)
 void k_reg_step(int alg, const float *a, float *out, int nx, int ny, int nz, float lambda,
-                cudaStream_t st);
+                cudaStream_t st, const float *lo = nullptr, const float *hi = nullptr);
+// Step scalars of a z-sharded solve (sum[0]: the value the ranks
+// all-reduce between stages).
+enum ShardOp { SH_LOCAL = 0, SH_INIT = 1, SH_ALPHA = 2, SH_BETA = 3 };
+void k_shard_scalars(int op, const double *p1, int n1, const double *p2, int n2, double *sum,
+                     double *s, double *norms, cudaStream_t st);
+// lo / hi = the first / last z plane of a slab ([x][y] each)
+void k_pack_edges(const float *a, int nx, int ny, int nz, float *lo, float *hi, cudaStream_t st);
 // out = L(a)
 void k_reg_apply(int alg, const float *a, float *out, int nx, int ny, int nz,
                  cudaStream_t st);

@@ -98,6 +98,53 @@ __global__ void cgls_scalars_kernel(int op, const double *p1, int n1, const doub
   }
 }
 
+// Step scalars of a solve whose volume is cut into slabs over several
+// ranks.  sum[0] is the one double the ranks all-reduce between stages:
+// SH_LOCAL writes this rank's FP64 sum of the partials (p1, then p2), the
+// other ops read the all-reduced total.  s[] as in cgls_scalars_kernel.
+__global__ void shard_scalars_kernel(int op, const double *p1, int n1, const double *p2, int n2,
+                                     double *sum, double *s, double *norms) {
+  __shared__ double red[kThreads / 32];
+  if (op == SH_LOCAL) {
+    const double a = block_sum_fixed(p1, n1, red);
+    const double b = p2 ? block_sum_fixed(p2, n2, red) : 0.0;
+    if (threadIdx.x == 0)
+      sum[0] = a + b;
+    return;
+  }
+  if (threadIdx.x != 0)
+    return;
+  const double t = sum[0];
+  switch (op) {
+  case SH_INIT:
+    s[0] = t;
+    s[1] = 0.0;
+    s[2] = 0.0;
+    s[3] = 0.0;
+    break;
+  case SH_ALPHA:
+    s[1] = (t > 0.0) ? s[0] / t : 0.0;
+    break;
+  case SH_BETA:
+    s[2] = (s[0] > 0.0) ? t / s[0] : 0.0;
+    s[0] = t;
+    if (norms)
+      norms[int(s[3])] = sqrt(t);
+    s[3] += 1.0;
+    break;
+  }
+}
+
+// The first and last z planes of a slab, [x][y] each: what the neighbouring
+// slabs take as their halo planes.
+__global__ void pack_edges_kernel(const float *__restrict__ a, int nxy, int nz, float *lo,
+                                  float *hi) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nxy; c += gridDim.x * blockDim.x) {
+    lo[c] = a[i64(c) * nz];
+    hi[c] = a[i64(c) * nz + nz - 1];
+  }
+}
+
 // blas.hpp:307-322 sum_axpy: y += a x, a rounded to float, unfused.
 __global__ void axpy_scalar_kernel(float *y, const float *__restrict__ x, i64 n, const double *s,
                                    int idx, float sign) {
@@ -131,11 +178,32 @@ __global__ void add_scaled_kernel(float *out, const float *in, const float *__re
 }
 
 // ---------------------------------------------------------- regularisers
+// A volume [x][y][z], optionally one slab of a volume cut along z: lo / hi
+// then hold the neighbouring slabs' adjacent planes (nx * ny, [x][y]),
+// which stand in for the planes k = -1 and k = nz; without them the z
+// neighbours mirror at the ends as in the reference.
 struct Vol {
   const float *a;
   int nx, ny, nz;
+  const float *lo = nullptr, *hi = nullptr;
   __device__ float at(int i, int j, int k) const {
+    if (k < 0)
+      return lo[i64(i) * ny + j];
+    if (k >= nz)
+      return hi[i64(i) * ny + j];
     return a[(i64(i) * ny + j) * nz + k];
+  }
+  // z neighbours: across a cut into the halo plane (a halo plane's own
+  // outer neighbour, which no result uses, reads the halo plane again)
+  __device__ int zdn(int k) const {
+    if (lo)
+      return k - 1 < -1 ? -1 : k - 1;
+    return (nz == 1) ? k : ((k - 1 < 0) ? k + 1 : k - 1);
+  }
+  __device__ int zup(int k) const {
+    if (hi)
+      return k + 1 > nz ? nz : k + 1;
+    return (nz == 1) ? k : ((k + 1 >= nz) ? k - 1 : k + 1);
   }
 };
 
@@ -174,8 +242,8 @@ __device__ float tv_d(const Vol &v, int i, int j, int k, int which) {
   const float y1 = __fsub_rn(v.at(i, mirror_up(j, v.ny), k), c);
   const float y0 = __fsub_rn(c, v.at(i, mirror_dn(j, v.ny), k));
   const float x0 = __fsub_rn(c, v.at(mirror_dn(i, v.nx), j, k));
-  const float z1 = __fsub_rn(v.at(i, j, mirror_up(k, v.nz)), c);
-  const float z0 = __fsub_rn(c, v.at(i, j, mirror_dn(k, v.nz)));
+  const float z1 = __fsub_rn(v.at(i, j, v.zup(k)), c);
+  const float z0 = __fsub_rn(c, v.at(i, j, v.zdn(k)));
   float d2x = minmod(y1, y0);
   float d2y = minmod(x1, x0);
   float d3x = minmod(z1, z0);
@@ -198,7 +266,7 @@ __device__ float tv_d(const Vol &v, int i, int j, int k, int which) {
 __device__ float tv_at(const Vol &v, int i, int j, int k) {
   const float dv1 = __fsub_rn(tv_d(v, i, j, k, 0), tv_d(v, mirror_dn(i, v.nx), j, k, 0));
   const float dv2 = __fsub_rn(tv_d(v, i, j, k, 1), tv_d(v, i, mirror_dn(j, v.ny), k, 1));
-  const float dv3 = __fsub_rn(tv_d(v, i, j, k, 2), tv_d(v, i, j, mirror_dn(k, v.nz), 2));
+  const float dv3 = __fsub_rn(tv_d(v, i, j, k, 2), tv_d(v, i, j, v.zdn(k), 2));
   return __fadd_rn(__fadd_rn(dv1, dv2), dv3);
 }
 
@@ -327,17 +395,26 @@ void k_add_scaled(float *out, const float *in, const float *d, i64 n, const doub
                   cudaStream_t st) {
   add_scaled_kernel<<<grid_for(n), kThreads, 0, st>>>(out, in, d, n, s);
 }
+void k_shard_scalars(int op, const double *p1, int n1, const double *p2, int n2, double *sum,
+                     double *s, double *norms, cudaStream_t st) {
+  shard_scalars_kernel<<<1, kThreads, 0, st>>>(op, p1, n1, p2, n2, sum, s, norms);
+}
+void k_pack_edges(const float *a, int nx, int ny, int nz, float *lo, float *hi, cudaStream_t st) {
+  const int nxy = nx * ny;
+  pack_edges_kernel<<<grid_for(nxy), kThreads, 0, st>>>(a, nxy, nz, lo, hi);
+}
 void k_reg_accumulate(int alg, const float *a, float *acc, int nx, int ny, int nz, float lambda,
-                      double *partials, int nblocks, cudaStream_t st) {
-  Vol v{a, nx, ny, nz};
+                      double *partials, int nblocks, cudaStream_t st, const float *lo,
+                      const float *hi) {
+  Vol v{a, nx, ny, nz, lo, hi};
   if (alg == 3)
     reg_accumulate_kernel<3><<<nblocks, kThreads, 0, st>>>(v, acc, lambda, partials);
   else
     reg_accumulate_kernel<4><<<nblocks, kThreads, 0, st>>>(v, acc, lambda, partials);
 }
 void k_reg_step(int alg, const float *a, float *out, int nx, int ny, int nz, float lambda,
-                cudaStream_t st) {
-  Vol v{a, nx, ny, nz};
+                cudaStream_t st, const float *lo, const float *hi) {
+  Vol v{a, nx, ny, nz, lo, hi};
   const i64 n = i64(nx) * ny * nz;
   if (alg == 3)
     reg_step_kernel<3><<<grid_for(n), kThreads, 0, st>>>(v, out, lambda);

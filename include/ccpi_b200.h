@@ -314,6 +314,46 @@ int ccpi_session_run(ccpi_session *session, int niterations);
 int ccpi_session_finish(ccpi_session *session, double *h_norms);
 void ccpi_session_destroy(ccpi_session *session);
 
+/* A CGLS-family solve (CCPI_CGLS, CCPI_CGLS_TIKHONOV, CCPI_CGLS_TV) of one
+ * z slab of a parallel-beam volume that is cut into slabs over several
+ * ranks (the reference's MPI split of the volume into z blocks,
+ * Core/src/voxels.cpp:27-45; rows map to their own slices, so each rank
+ * projects its slab alone).  The plan is the slab's geometry (its rows, its
+ * slices).  The iteration of cgls.cpp:87-157 / :343-423 is run in stages;
+ * between two stages the caller makes the exchange the next stage needs:
+ *   SETUP     then all-reduce (sum) *d_sum; TV: swap halos
+ *   FORWARD   then all-reduce *d_sum
+ *   UPDATE    then TV: swap halos
+ *   BACKWARD  then all-reduce *d_sum
+ *   NEXT      then TV: swap halos; continue with FORWARD
+ * d_sum: one device double, written by SETUP / FORWARD / BACKWARD with this
+ * rank's FP64 partial sum and read back (all-reduced in place by the
+ * caller) by the next stage.  d_edges: 2 * nx * ny device floats, the
+ * slab's first and last z planes ([x][y]) after the stages marked "swap
+ * halos"; d_halo_lo / d_halo_hi: nx * ny device floats holding the
+ * neighbouring slabs' adjacent planes (the lower neighbour's last plane,
+ * the upper neighbour's first plane), or NULL at the volume's ends, where
+ * the TV stencil mirrors as in the reference (total_v.cpp:31-52).  One rank
+ * with no halos gives ccpi_solve's result bit for bit.  Stages are enqueued
+ * on `stream` and are not waited for; out-of-order stages are an error.
+ * finish (after NEXT): clamps d_x at zero, waits, returns the per-iteration
+ * |A^T r| of the whole volume. */
+typedef struct ccpi_shard ccpi_shard;
+enum {
+  CCPI_SHARD_SETUP = 0,
+  CCPI_SHARD_FORWARD = 1,
+  CCPI_SHARD_UPDATE = 2,
+  CCPI_SHARD_BACKWARD = 3,
+  CCPI_SHARD_NEXT = 4
+};
+int ccpi_shard_create(const ccpi_plan *plan, int alg, const float *d_sino, float *d_x,
+                      double regularize, int max_iterations, double *d_sum, float *d_edges,
+                      const float *d_halo_lo, const float *d_halo_hi, void *stream,
+                      ccpi_shard **shard);
+int ccpi_shard_stage(ccpi_shard *shard, int stage);
+int ccpi_shard_finish(ccpi_shard *shard, double *h_norms);
+void ccpi_shard_destroy(ccpi_shard *shard);
+
 /* ccpi_solve for callers that must not allocate device memory during a
  * solve: a host that owns all device memory through its own pool, or a
  * loop running other streams that cannot take the device-wide

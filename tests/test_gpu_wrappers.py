@@ -32,7 +32,7 @@ def test_pb_projectors_fixture(cuda):
 
 
 @pytest.mark.parametrize("shape,na,ppv", [((30, 22, 12), 25, 1), ((18, 26, 10), 19, 2),
-                                          ((16, 16, 5), 40, 1)])
+                                          ((16, 16, 8), 40, 1)])
 def test_pb_forward_project_vs_reference(shape, na, ppv, cuda):
     if not O.reference_available():
         pytest.skip("oracle/_ref/libccpi_ref.so not built")
@@ -44,6 +44,30 @@ def test_pb_forward_project_vs_reference(shape, na, ppv, cuda):
     ref = O.ref_pb_forward_project(vol, ang, ppv)
     assert got.shape == ref.shape
     assert np.array_equal(got, ref), max_rel(got, ref)
+
+
+def test_pb_forward_project_padded_rows(cuda):
+    """A volume whose height is not a multiple of the row alignment: the
+    detector gets padding rows (instruments.cpp:35-64) that map to slices
+    outside the volume.  The reference then reads outside the voxel column
+    (the neighbouring column's voxels, or memory outside the volume at the
+    array's ends; p2D.cpp:63-213 has no bound check); this library projects
+    nothing there.  Rows that map into the volume equal the reference bit
+    for bit, padding rows are zero."""
+    if not O.reference_available():
+        pytest.skip("oracle/_ref/libccpi_ref.so not built")
+    from ccpi.reconstruction.parallelbeam import alg
+    rng = np.random.default_rng(61)
+    vol = rng.random((16, 16, 5)).astype(np.float32)
+    ang = np.sort(rng.uniform(0.0, 180.0, 40)).astype(np.float32)
+    got = alg.pb_forward_project(vol, ang, 1)
+    ref = O.ref_pb_forward_project(vol, ang, 1)
+    assert got.shape == ref.shape == (40, 8, 16)
+    nvp, voff = O.v_alignment(5, 1)
+    assert (nvp, voff) == (8, 1)
+    inside = slice(voff, voff + 5)
+    assert np.array_equal(got[:, inside, :], ref[:, inside, :])
+    assert not got[:, :voff, :].any() and not got[:, voff + 5:, :].any()
 
 
 @pytest.mark.parametrize("na,nv,nh,cor,ppv", [(21, 8, 30, 0.0, 1), (17, 6, 27, 14.75, 1),
