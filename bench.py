@@ -77,9 +77,8 @@ def parse():
                     choices=["cone-cgls", "sirt", "uneven", "autograd", "cone-projectors"],
                     help="cone-cgls: the default line; the others print their own line")
     ap.add_argument("--cone-n", type=int, default=CN,
-                    help="cone-projectors: grid edge (512: the CGLS workload's projectors; 256: "
-                         "360 angles onto a 384^2 detector at 1.6 mm, 2 mm voxels, for profiler "
-                         "captures)")
+                    help="cone grid edge (512: the CGLS workload; 256: 360 angles onto a 384^2 "
+                         "detector at 1.6 mm, 2 mm voxels, for profiler captures)")
     args = ap.parse_args()
     if args.small:
         g = globals()
@@ -196,6 +195,13 @@ def ellipsoid_phantom(n, count, axes, seed):
             acc = u * u if acc is None else acc + u * u
         vol[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] += (acc <= 1.0).astype(np.float32) * den
     return vol
+
+
+def cone_geometry(n):
+    """(grid edge, voxel mm, angles, detector edge, pixel mm) of the cone
+    workload (n = 512) or its 256^3 profiling copy (360 angles onto a 384^2
+    detector at 1.6 mm, 2 mm voxels: the same voxel shadow in pixels)."""
+    return (CN, 1.0, CNA, CND, CPIX) if n == CN else (n, 2.0 * 256 / n, 360, 384, 1.6)
 
 
 def cone_angles(count=CNA, every=1):
@@ -423,13 +429,15 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
     from ccpi.reconstruction import _native as N
     from ccpi.reconstruction.conebeam import alg as CA
     from ccpi.reconstruction.device import Session, cone_plan
-    plan = cone_plan(CN, 1.0, CNA, CND, CPIX, CS2O, CO2D)
-    vol_np = ellipsoid_phantom(CN, 40, (10.0, 120.0), seed=3 + rank)
+    n, vs, na, nd, px = cone_geometry(args.cone_n)
+    full = n == CN
+    plan = cone_plan(n, vs, na, nd, px, CS2O, CO2D)
+    vol_np = ellipsoid_phantom(n, 40, (10.0 * n / CN, 120.0 * n / CN), seed=3 + rank)
     clean = plan.forward(torch.from_numpy(vol_np).to(dev))
     mu = 3.0 / float(clean.max())
     sino = poisson_log_torch(torch, clean, mu, 5.0e3, 3 + rank)
     del clean
-    V, P = CN ** 3, CNA * CND * CND
+    V, P = n ** 3, na * nd * nd
     stream = torch.cuda.current_stream(dev)
 
     # ---- graph-captured CGLS (the headline), data resident
@@ -472,10 +480,9 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
     host_s = torch.empty(sino.shape, dtype=torch.float32, pin_memory=True)
     host_s.copy_(sino)
     host_x = torch.empty(plan.shape, dtype=torch.float32, pin_memory=True)
-    h, v = cone_detector()
-    ang = cone_angles()
+    ang, h, v = (np.asarray(a, np.float64) for a in plan._arrays)
     geo = dict(source=(-CS2O, 0.0, 0.0), detector_x=CO2D, h_pixels=h, v_pixels=v, angles=ang,
-               grid_offset=(-CN / 2.0,) * 3, voxel_size=(1.0,) * 3, shape=(CN,) * 3)
+               grid_offset=(-n * vs / 2.0,) * 3, voxel_size=(vs,) * 3, shape=(n,) * 3)
     del sino, x
     torch.cuda.empty_cache()
 
@@ -495,7 +502,7 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
 
     fp64 = None
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and full:
         if not args.no_fp64:
             fp64 = cone_fp64_check(torch, dev)
         if not args.no_cpu:
@@ -511,9 +518,12 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_it,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": CONE_WORKLOAD, "solver": "CGLS", "grid": [CN, CN, CN],
-                   "angles": CNA, "detector": [CND, CND], "mu": mu,
-                   "l2": "inputs larger than L2 (sinogram 1.7 GB, volume 537 MB)",
+        "config": {"workload": CONE_WORKLOAD if full else
+                   f"cone-beam CGLS, {n}^3 ellipsoid phantom, {na} angles, {nd}^2 detector "
+                   f"(profiling size)", "solver": "CGLS", "grid": [n, n, n],
+                   "angles": na, "detector": [nd, nd], "mu": mu,
+                   "l2": "inputs larger than L2 (sinogram %.0f MB, volume %.0f MB)"
+                         % (4.0 * P / 1e6, 4.0 * V / 1e6),
                    "form": "one CUDA graph per iteration",
                    "multi_gpu": "replicas: each rank solves its own problem"},
         "fp_ms": 1000.0 * t_fp, "bp_ms": 1000.0 * t_bp,
@@ -771,7 +781,7 @@ def run_uneven(args):
     import numpy as np
     import torch
 
-    from ccpi.reconstruction.device import pack_parallel, parallel_api_plan, solve_batched
+    from ccpi.reconstruction.device import Session, pack_parallel, parallel_api_plan, solve_batched
     from ccpi.reconstruction.parallelbeam import alg as A
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
@@ -808,7 +818,19 @@ def run_uneven(args):
             tp += cuda_time(torch, lambda: plans[i].solve(alg, sinos[i], y, niter, lams[i],
                                                          plain=True))
         t_plain = tp * len(plans) / len(sample)
-        res[name] = {"batched_s": t, "plain_s": t_plain}
+        # the kernels alone: every problem's graph-captured iteration timed
+        # on its own (data resident), summed over the 64 problems; no
+        # batched form of the same kernels can beat this sum by more than
+        # the overlap of problems too small to fill the GPU
+        t_kern = 0.0
+        for i, pl in enumerate(plans):
+            y = torch.zeros(pl.shape, device=dev)
+            sess = Session(pl, alg, sinos[i], y, 3, lams[i])
+            sess.run(1)
+            t_kern += cuda_time(torch, lambda: sess.run(2)) / 2.0
+            sess.finish()
+            sess.close()
+        res[name] = {"batched_s": t, "plain_s": t_plain, "kernels_s": t_kern * niter}
     clk = clocks.stop()
     # e2e through the host-buffer batched call (Tikhonov)
     t0 = time.perf_counter()
@@ -828,6 +850,8 @@ def run_uneven(args):
          "autotune": {"seconds": t_tune, "bp_slices_per_lane_chosen": vw_counts}},
         tv_iter_per_s=niter / res["cgls_TVreg"]["batched_s"],
         plain_iter_per_s={k: niter / v["plain_s"] for k, v in res.items()},
+        kernels_only_iter_per_s={k: niter / v["kernels_s"] for k, v in res.items()},
+        plain_over_kernels_only={k: v["plain_s"] / v["kernels_s"] for k, v in res.items()},
         batched_over_plain={k: v["plain_s"] / v["batched_s"] for k, v in res.items()},
         roofline={"bound": "hbm", "kernel": "one regularised CGLS iteration of the batch",
                   "achieved": it_bytes / (t_tik / niter) / 1e9, "peak": peak, "unit": "GB/s",
@@ -937,10 +961,7 @@ def run_cone_projectors(args):
     from ccpi.reconstruction.device import cone_plan
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    if args.cone_n == CN:
-        n, vs, na, nd, px = CN, 1.0, CNA, CND, CPIX
-    else:
-        n, vs, na, nd, px = args.cone_n, 2.0 * 256 / args.cone_n, 360, 384, 1.6
+    n, vs, na, nd, px = cone_geometry(args.cone_n)
     plan = cone_plan(n, vs, na, nd, px, CS2O, CO2D)
     vol = torch.from_numpy(ellipsoid_phantom(n, 40, (10.0 * n / CN, 120.0 * n / CN), seed=3)).to(dev)
     sino = plan.forward(vol)

@@ -82,6 +82,8 @@ def _load():
     lib.ccpi_plan_pixels.restype = ctypes.c_longlong
     lib.ccpi_forward.argtypes = [_vp, _vp, _vp, _vp]
     lib.ccpi_backward.argtypes = [_vp, _vp, _vp, _vp]
+    lib.ccpi_forward_batch.argtypes = [_vp, _c_int, _vp, _vp, _vp]
+    lib.ccpi_backward_batch.argtypes = [_vp, _c_int, _vp, _vp, _vp]
     lib.ccpi_solve_workspace_bytes.argtypes = [_vp, _c_int, _c_int]
     lib.ccpi_solve_workspace_bytes.restype = _sz
     lib.ccpi_solve.argtypes = [_vp, _c_int, _vp, _vp, _c_int, _c_dbl, _vp, _c_int, _vp, _sz, _vp]

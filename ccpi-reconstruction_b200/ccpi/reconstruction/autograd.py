@@ -9,7 +9,8 @@ stream; torch only supplies the tensors.
 
 Shapes: a volume is ``(..., nx, ny, nz)`` and a sinogram ``(..., n_angles,
 n_h, n_v)`` (the library's internal layout, v fastest).  Leading batch
-dimensions are projected one item per launch.
+dimensions are projected together (``ccpi_forward_batch`` /
+``ccpi_backward_batch``: one launch per direction for cone beam).
 """
 from __future__ import annotations
 
@@ -18,7 +19,7 @@ import torch
 from .device import Plan
 
 
-def _batched(fn, plan: Plan, src: torch.Tensor, in_shape, out_shape):
+def _batched(fwd, plan: Plan, src: torch.Tensor, in_shape, out_shape):
     if tuple(src.shape[-3:]) != tuple(in_shape):
         raise ValueError(f"expected trailing shape {tuple(in_shape)}, got {tuple(src.shape)}")
     lead = src.shape[:-3]
@@ -26,19 +27,18 @@ def _batched(fn, plan: Plan, src: torch.Tensor, in_shape, out_shape):
     if not flat.is_contiguous():
         flat = flat.contiguous()
     out = torch.empty((flat.shape[0],) + tuple(out_shape), device=src.device, dtype=torch.float32)
-    for i in range(flat.shape[0]):
-        fn(flat[i], out[i])
+    (plan.forward_batch if fwd else plan.backward_batch)(flat, out)
     return out.reshape(tuple(lead) + tuple(out_shape))
 
 
 def forward_project(plan: Plan, vol: torch.Tensor) -> torch.Tensor:
     """A x for a volume or a batch of volumes (no autograd)."""
-    return _batched(plan.forward, plan, vol, plan.shape, plan.sino_shape)
+    return _batched(True, plan, vol, plan.shape, plan.sino_shape)
 
 
 def back_project(plan: Plan, sino: torch.Tensor) -> torch.Tensor:
     """A^T y for a sinogram or a batch of sinograms (no autograd)."""
-    return _batched(plan.backward, plan, sino, plan.sino_shape, plan.shape)
+    return _batched(False, plan, sino, plan.sino_shape, plan.shape)
 
 
 class ProjectFunction(torch.autograd.Function):

@@ -99,6 +99,23 @@ class Plan:
                 "ccpi_backward")
         return out
 
+    def _batch(self, name, src, out, in_shape, out_shape):
+        if src.dim() != 4 or out.dim() != 4 or src.shape[0] != out.shape[0]:
+            raise ValueError(f"{name}: expected (n, ...) input and output of one batch size")
+        self._check(src, in_shape, "input")
+        self._check(out, out_shape, "output")
+        N.check(getattr(N.lib, name)(self._h, int(src.shape[0]), ctypes.c_void_p(src.data_ptr()),
+                                     ctypes.c_void_p(out.data_ptr()), self._stream(src)), name)
+        return out
+
+    def forward_batch(self, vol, out):
+        """out[b] = A vol[b] for a (n, nx, ny, nz) batch (``ccpi_forward_batch``)."""
+        return self._batch("ccpi_forward_batch", vol, out, self.shape, self.sino_shape)
+
+    def backward_batch(self, sino, out):
+        """out[b] = A^T sino[b] for a (n, n_angles, n_h, n_v) batch."""
+        return self._batch("ccpi_backward_batch", sino, out, self.sino_shape, self.shape)
+
     def workspace_bytes(self, alg, niterations):
         return int(N.lib.ccpi_solve_workspace_bytes(self._h, int(alg), int(niterations)))
 

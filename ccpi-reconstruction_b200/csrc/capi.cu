@@ -882,6 +882,51 @@ int ccpi_backward(const ccpi_plan *plan, const float *d_sino, float *d_volume, v
   return ccpi::cuda_ok(cudaGetLastError(), "ccpi_backward") ? 0 : 2;
 }
 
+// n projections of one plan: cone beam in one launch per direction (the
+// rays' walks and the columns' band limits are shared by the batch),
+// parallel beam one launch per item.
+static int project_batch(const char *what, const ccpi_plan *plan, int n, const float *in,
+                         float *out, bool fwd, void *stream) {
+  if (!plan || !in || !out || n < 0) {
+    set_error(std::string(what) + ": null argument or negative batch");
+    return 1;
+  }
+  const i64 nin = fwd ? plan->nvox : plan->npix, nout = fwd ? plan->npix : plan->nvox;
+  if (!aligned16(in) || !aligned16(out) ||
+      (n > 1 && ((nin * 4) % 16 != 0 || (nout * 4) % 16 != 0))) {
+    set_error(std::string(what) + ": every item must start on a 16-byte boundary");
+    return 1;
+  }
+  const cudaStream_t st = cudaStream_t(stream);
+  ccpi::Epi e{};
+  if (plan->g.kind == CCPI_CONE && n > 0) {
+    const int rc = fwd ? ccpi::cb_forward(plan->g, in, out, ccpi::EPI_STORE, e, plan->hrange,
+                                          plan->fp_grid, st, n)
+                       : ccpi::cb_backward(plan->g, in, out, ccpi::EPI_STORE, e, plan->err, st, n);
+    if (rc)
+      return 3;
+  } else {
+    for (int b = 0; b < n; b++) {
+      const float *src = in + i64(b) * nin;
+      float *dst = out + i64(b) * nout;
+      if (fwd ? ccpi::forward(plan, src, dst, ccpi::EPI_STORE, e, st)
+              : ccpi::backward(plan, src, dst, ccpi::EPI_STORE, e, st))
+        return 3;
+    }
+  }
+  return ccpi::cuda_ok(cudaGetLastError(), what) ? 0 : 2;
+}
+
+int ccpi_forward_batch(const ccpi_plan *plan, int n, const float *d_volumes, float *d_sinos,
+                       void *stream) {
+  return project_batch("ccpi_forward_batch", plan, n, d_volumes, d_sinos, true, stream);
+}
+
+int ccpi_backward_batch(const ccpi_plan *plan, int n, const float *d_sinos, float *d_volumes,
+                        void *stream) {
+  return project_batch("ccpi_backward_batch", plan, n, d_sinos, d_volumes, false, stream);
+}
+
 size_t ccpi_solve_workspace_bytes(const ccpi_plan *plan, int alg, int niterations) {
   return plan ? ccpi::solve_workspace_bytes(plan, alg, niterations) : 0;
 }

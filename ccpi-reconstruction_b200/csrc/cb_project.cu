@@ -196,11 +196,13 @@ constexpr int kFpWarps = 4;
 __host__ __device__ inline int cb_vz_floats(int nz) { return (nz + 1 + 3) & ~3; }
 
 // RPL = detector rows per lane per pass (a pass covers 32 * RPL rows);
-// FULL: nv is a multiple of 32 * RPL (no idle rows).
+// FULL: nv is a multiple of 32 * RPL (no idle rows).  nb volumes (one
+// after another) share each ray's walk and row regimes; EPI_STORE when
+// nb > 1.
 template <int EPI, int RPL, bool FULL>
 __global__ void __launch_bounds__(kFpWarps * 32)
-    cb_fp_kernel(Geom g, const float *__restrict__ vol, float *__restrict__ pix, Epi e,
-                 const int2 *__restrict__ hrange, int cap) {
+    cb_fp_kernel(Geom g, const float *__restrict__ vol0, float *__restrict__ pix0, Epi e,
+                 const int2 *__restrict__ hrange, int cap, int nb) {
   extern __shared__ unsigned char smem_raw[];
   const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float *svz = reinterpret_cast<float *>(smem_raw);
@@ -282,6 +284,10 @@ __global__ void __launch_bounds__(kFpWarps * 32)
     // Rows, RPL per lane per pass.  Cells [1, mfast) have every row inside
     // the slab (c2D.cpp:99-145); the rest take the edge rules (:146-190).
     const int mfast = min(ncom, n);
+    for (int b = 0; b < nb; b++) {
+    // batch item b: its volume and its sinogram
+    const float *__restrict__ vol = vol0 + i64(b) * g.nx * g.ny * g.nz;
+    float *__restrict__ pix = pix0 + i64(b) * g.na * g.nh * g.nv;
     for (int vb = 0; vb < g.nv; vb += 32 * RPL) {
       float acc[RPL], dzv[RPL], izv[RPL];
       bool vok[RPL], below[RPL];
@@ -424,6 +430,7 @@ __global__ void __launch_bounds__(kFpWarps * 32)
         }
       }
     }
+    } // batch items
     __syncwarp();
   }
   if (EPI == EPI_NORM) {
@@ -756,8 +763,8 @@ __device__ __forceinline__ void cb_ga_mark(int *f, int kp, int k, int v, int nz)
 // so a staged row is one load and no multiply.  ST rays per stage.
 template <int EPI, int NZT, int RMAX, bool PRE, int ST>
 __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
-    cb_bp_gather(Geom g, const float *__restrict__ pix, float *__restrict__ vol, Epi e,
-                 int *err) {
+    cb_bp_gather(Geom g, const float *__restrict__ pix0, float *__restrict__ vol0, Epi e,
+                 int *err, int nbatch) {
   static_assert(ST <= kGaStageMax, "stage too large");
   extern __shared__ unsigned char smem_raw[];
   int *W = reinterpret_cast<int *>(smem_raw);
@@ -813,10 +820,6 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
   const int lo_end = min(mid, max_v);         // lower band rows [min_v, lo_end)
   const int up_begin = max(mid, min_v);       // upper band rows [up_begin, max_v)
   const float pzbz = g.pzbz, pzbz1 = g.pzbz1, inv_dz = g.inv_dz;
-  float acc[NZT];
-#pragma unroll
-  for (int q = 0; q < NZT; q++)
-    acc[q] = 0.0f;
   // this thread's band rows v = min_v + tid + r * 256 are the same for every
   // ray: their z tables stay in registers (sd: delta_z of v, sp: of v - 1,
   // si: inv_delz of v)
@@ -830,6 +833,15 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
     rsi[r] = in ? siz[v] : 0.0f;
   }
   const float sd_first = nb > 0 ? sdz[min_v] : 0.0f, sd_last = nb > 0 ? sdz[max_v - 1] : 0.0f;
+  double ssq = 0.0;
+  // nbatch sinograms (one after another) share the column's band limits
+  for (int bi = 0; bi < nbatch; bi++) {
+  const float *__restrict__ pix = pix0 + i64(bi) * g.na * g.nh * nv;
+  float *__restrict__ vol = vol0 + i64(bi) * g.nx * g.ny * nz;
+  float acc[NZT];
+#pragma unroll
+  for (int q = 0; q < NZT; q++)
+    acc[q] = 0.0f;
 
   // ---- band rows of every ray (c2D.cpp:680-713)
   for (int ac = 0; nb > 0 && ac < g.na; ac += kGaChunk) {
@@ -1038,9 +1050,6 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
       __syncthreads();
     }
   }
-  if (tid == 0 && s_ovf)
-    atomicExch(err, 2);
-  double ssq = 0.0;
   const i64 base = i64(col) * nz;
 #pragma unroll
   for (int q = 0; q < NZT; q++) {
@@ -1060,6 +1069,9 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
     }
     vol[base + K] = o;
   }
+  } // batch items
+  if (tid == 0 && s_ovf)
+    atomicExch(err, 2);
   if (EPI == EPI_NORM) {
     __shared__ double red[kGaThreads / 32];
     const double t = cta_sum<kGaThreads / 32>(ssq, red);
@@ -1096,14 +1108,14 @@ int cb_fp_rpl(int nv) {
 
 template <int EPI>
 void launch_cb_fp(const Geom &g, const float *vol, float *pix, const Epi &e, const int2 *hrange,
-                  int grid, cudaStream_t st) {
+                  int grid, cudaStream_t st, int nb) {
   const size_t smem = cb_fp_smem(g);
   const int cap = g.nx + g.ny + 2;
   const int r = (g.tune_rpl == 4 || g.tune_rpl == 8 || g.tune_rpl == 12) ? g.tune_rpl
                                                                           : cb_fp_rpl(g.nv);
   const bool full = g.nv % (32 * r) == 0;
 #define CB_FP_GO(R, F)                                                                     \
-  cb_fp_kernel<EPI, R, F><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap)
+  cb_fp_kernel<EPI, R, F><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap, nb)
   if (r == 12)
     full ? CB_FP_GO(12, true) : CB_FP_GO(12, false);
   else if (r == 8)
@@ -1177,19 +1189,19 @@ int cb_prepare(const Geom &g) {
 }
 
 int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
-               const int2 *hrange, int grid, cudaStream_t st) {
+               const int2 *hrange, int grid, cudaStream_t st, int nb) {
   switch (mode) {
   case EPI_STORE:
-    launch_cb_fp<EPI_STORE>(g, vol, pix, e, hrange, grid, st);
+    launch_cb_fp<EPI_STORE>(g, vol, pix, e, hrange, grid, st, nb);
     break;
   case EPI_NORM:
-    launch_cb_fp<EPI_NORM>(g, vol, pix, e, hrange, grid, st);
+    launch_cb_fp<EPI_NORM>(g, vol, pix, e, hrange, grid, st, nb);
     break;
   case EPI_SIRT:
-    launch_cb_fp<EPI_SIRT>(g, vol, pix, e, hrange, grid, st);
+    launch_cb_fp<EPI_SIRT>(g, vol, pix, e, hrange, grid, st, nb);
     break;
   case EPI_MLEM:
-    launch_cb_fp<EPI_MLEM>(g, vol, pix, e, hrange, grid, st);
+    launch_cb_fp<EPI_MLEM>(g, vol, pix, e, hrange, grid, st, nb);
     break;
   default:
     return 1;
@@ -1210,14 +1222,14 @@ __global__ void cb_prescale_kernel(const float *__restrict__ in, float *__restri
 
 template <int EPI, bool PRE, int ST>
 void launch_cb_ga(const Geom &g, int nzt, int rmax, const float *pix, float *vol, const Epi &e,
-                  int *err, cudaStream_t st) {
+                  int *err, cudaStream_t st, int nbatch) {
   const int ncol = g.nx * g.ny;
   const size_t gsm = cb_bp_gather_smem(g);
 #define CB_GA_GO(Z)                                                                        \
-  (rmax == 1   ? cb_bp_gather<EPI, Z, 1, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err) \
-   : rmax == 2 ? cb_bp_gather<EPI, Z, 2, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err) \
-   : rmax == 3 ? cb_bp_gather<EPI, Z, 3, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err) \
-               : cb_bp_gather<EPI, Z, 4, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err))
+  (rmax == 1   ? cb_bp_gather<EPI, Z, 1, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err, nbatch) \
+   : rmax == 2 ? cb_bp_gather<EPI, Z, 2, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err, nbatch) \
+   : rmax == 3 ? cb_bp_gather<EPI, Z, 3, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err, nbatch) \
+               : cb_bp_gather<EPI, Z, 4, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err, nbatch))
   if (nzt == 1)
     CB_GA_GO(1);
   else if (nzt == 2)
@@ -1229,28 +1241,29 @@ void launch_cb_ga(const Geom &g, int nzt, int rmax, const float *pix, float *vol
 
 template <int EPI>
 void launch_cb_bp(const Geom &g, const float *pix, float *vol, const Epi &e, int *err,
-                  cudaStream_t st) {
+                  cudaStream_t st, int nbatch) {
   const int ncol = g.nx * g.ny;
   const int nzt = cb_bp_gather_nzt(g), rmax = cb_bp_gather_rmax(g);
   if (nzt && e.pre) {
-    launch_cb_ga<EPI, true, CB_GA_STAGE_PRE>(g, nzt, rmax, pix, vol, e, err, st);
+    launch_cb_ga<EPI, true, CB_GA_STAGE_PRE>(g, nzt, rmax, pix, vol, e, err, st, nbatch);
     return;
   }
   switch (nzt) {
   case 1:
   case 2:
   case 4:
-    launch_cb_ga<EPI, false, CB_GA_STAGE>(g, nzt, rmax, pix, vol, e, err, st);
+    launch_cb_ga<EPI, false, CB_GA_STAGE>(g, nzt, rmax, pix, vol, e, err, st, nbatch);
     break;
   default:
-    cb_bp_kernel<EPI><<<ncol, kBpThreads, cb_bp_atomic_smem(g), st>>>(g, pix, vol, e, err);
+    // columns taller than the gather handles: one launch per batch item
+    for (int b = 0; b < nbatch; b++)
+      cb_bp_kernel<EPI><<<ncol, kBpThreads, cb_bp_atomic_smem(g), st>>>(
+          g, pix + i64(b) * g.na * g.nh * g.nv, vol + i64(b) * g.nx * g.ny * g.nz, e, err);
   }
 }
 } // namespace
 
-bool cb_bp_takes_prescaled(const Geom &g) {
-  return cb_bp_gather_nzt(g) != 0 && i64(g.na) * g.nh < (i64(1) << 31);
-}
+bool cb_bp_takes_prescaled(const Geom &g) { return cb_bp_gather_nzt(g) != 0; }
 
 void cb_prescale(const Geom &g, const float *in, float *out, cudaStream_t st) {
   const i64 per = i64(g.nh) * g.nv, n = i64(g.na) * per;
@@ -1259,19 +1272,19 @@ void cb_prescale(const Geom &g, const float *in, float *out, cudaStream_t st) {
 }
 
 int cb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
-                int *err, cudaStream_t st) {
+                int *err, cudaStream_t st, int nbatch) {
   switch (mode) {
   case EPI_STORE:
-    launch_cb_bp<EPI_STORE>(g, pix, vol, e, err, st);
+    launch_cb_bp<EPI_STORE>(g, pix, vol, e, err, st, nbatch);
     break;
   case EPI_NORM:
-    launch_cb_bp<EPI_NORM>(g, pix, vol, e, err, st);
+    launch_cb_bp<EPI_NORM>(g, pix, vol, e, err, st, nbatch);
     break;
   case EPI_SIRT:
-    launch_cb_bp<EPI_SIRT>(g, pix, vol, e, err, st);
+    launch_cb_bp<EPI_SIRT>(g, pix, vol, e, err, st, nbatch);
     break;
   case EPI_MLEM:
-    launch_cb_bp<EPI_MLEM>(g, pix, vol, e, err, st);
+    launch_cb_bp<EPI_MLEM>(g, pix, vol, e, err, st, nbatch);
     break;
   default:
     return 1;

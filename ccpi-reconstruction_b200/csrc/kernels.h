@@ -16,10 +16,12 @@ int pb_bp_tiles(const Geom &g);
 int cb_prepare(const Geom &g);
 size_t cb_fp_smem(const Geom &g);
 size_t cb_bp_smem(const Geom &g);
+// nb / nbatch: that many volumes and sinograms one after another, one launch
+// (EPI_STORE); the walk, row regimes and band limits are shared
 int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi &e,
-               const int2 *hrange, int grid, cudaStream_t st);
+               const int2 *hrange, int grid, cudaStream_t st, int nb = 1);
 int cb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
-                int *err, cudaStream_t st);
+                int *err, cudaStream_t st, int nbatch = 1);
 // The cone back projector accepts a sinogram pre-scaled by d_conv (Epi::pre)
 // for this geometry; cb_prescale writes that scaled copy.
 bool cb_bp_takes_prescaled(const Geom &g);

@@ -271,6 +271,17 @@ int ccpi_forward(const ccpi_plan *plan, const float *d_volume, float *d_sino,
 /* vol = A^T sino (overwritten). */
 int ccpi_backward(const ccpi_plan *plan, const float *d_sino, float *d_volume,
                   void *stream);
+/* The same for n items of one plan stored one after another (volumes
+ * nx*ny*nz floats apart, sinograms n_angles*n_h*n_v apart), e.g. a batch
+ * of volumes under torch autograd.  Cone beam runs one launch per
+ * direction, the batch sharing each ray's xy walk and each column's ray
+ * list (f2D / b2D, Core/src/c2D.cpp:469-625, :948-1119, called once per
+ * item in the reference); parallel beam one launch per item.  Every item
+ * must start on a 16-byte boundary. */
+int ccpi_forward_batch(const ccpi_plan *plan, int n, const float *d_volumes, float *d_sinos,
+                       void *stream);
+int ccpi_backward_batch(const ccpi_plan *plan, int n, const float *d_sinos, float *d_volumes,
+                        void *stream);
 
 /* Device bytes ccpi_solve needs as workspace for `alg` and `niterations`. */
 size_t ccpi_solve_workspace_bytes(const ccpi_plan *plan, int alg,
