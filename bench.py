@@ -536,7 +536,11 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
                      "frac": bp_bytes / t_bp / 1e9 / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bp_bytes,
                      "traffic": traffic,
-                     "traffic_frac": (bp_bytes / traffic) if traffic else None},
+                     # DRAM bytes of one ncu capture of the same launch,
+                     # moved in this run's launch time
+                     "traffic_gbs": (traffic / t_bp / 1e9) if traffic else None,
+                     "traffic_frac": (traffic / t_bp / 1e9 / peak) if traffic else None,
+                     "algorithmic_over_traffic": (bp_bytes / traffic) if traffic else None},
         "iteration_roofline": {"achieved": it_bytes / t_it / 1e9, "unit": "GB/s",
                                "frac": it_bytes / t_it / 1e9 / peak,
                                "algorithmic_bytes_per_iteration": it_bytes},
@@ -546,7 +550,9 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
                 "call": "ccpi_reconstruct(cone geometry, CGLS, %d iterations), pinned host "
                         "sinogram and volume; plan, upload, set-up and download inside"
                         % args.steps},
-        "gpu_launches": 6 * args.steps,
+        # per iteration: forward, alpha, residual update, d_conv pre-scale,
+        # back projection, beta, x/d update
+        "gpu_launches": 7 * args.steps,
         "clocks": clk,
         "residual_norms": [float(n_) for n_ in norms[-3:]],
         "fp64_oracle": fp64,

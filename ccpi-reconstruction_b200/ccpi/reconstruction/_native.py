@@ -74,6 +74,7 @@ def _load():
     lib.ccpi_reconstruct.argtypes = [P(Geometry), _c_int, _vp, _c_int, _c_dbl, _vp, _vp]
     lib.ccpi_plan_create.argtypes = [P(Geometry), P(_vp)]
     lib.ccpi_plan_autotune.argtypes = [_vp, _vp, _i32p]
+    lib.ccpi_plan_set_cone_backprojector.argtypes = [_vp, _c_int]
     lib.ccpi_plan_destroy.argtypes = [_vp]
     lib.ccpi_plan_destroy.restype = None
     lib.ccpi_plan_voxels.argtypes = [_vp]

@@ -56,6 +56,12 @@ class Plan:
                                          chosen), "ccpi_plan_autotune")
         return int(chosen[0]), int(chosen[1])
 
+    def set_cone_backprojector(self, scatter):
+        """Cone beam: 1 = ray-driven scatter back projector (float atomics),
+        0 = the deterministic voxel gather (``ccpi_plan_set_cone_backprojector``)."""
+        N.check(N.lib.ccpi_plan_set_cone_backprojector(self._h, int(bool(scatter))),
+                "ccpi_plan_set_cone_backprojector")
+
     def close(self):
         if self._h:
             N.lib.ccpi_plan_destroy(self._h)

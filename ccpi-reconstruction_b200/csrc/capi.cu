@@ -846,6 +846,15 @@ int ccpi_plan_autotune(ccpi_plan *plan, void *stream, int chosen[2]) {
   return ccpi::plan_autotune(plan, cudaStream_t(stream), chosen);
 }
 
+int ccpi_plan_set_cone_backprojector(ccpi_plan *plan, int scatter) {
+  ccpi::g_last_error.clear();
+  if (!plan) {
+    set_error("ccpi_plan_set_cone_backprojector: null plan");
+    return 1;
+  }
+  return ccpi::set_cone_backprojector(plan, scatter);
+}
+
 long long ccpi_plan_voxels(const ccpi_plan *plan) { return plan ? plan->nvox : 0; }
 long long ccpi_plan_pixels(const ccpi_plan *plan) { return plan ? plan->npix : 0; }
 

@@ -195,6 +195,71 @@ constexpr int kFpWarps = 4;
 // projector's shared memory (nz + 1 entries, rounded up to 4).
 __host__ __device__ inline int cb_vz_floats(int nz) { return (nz + 1 + 3) & ~3; }
 
+// Row regimes of a walked ray (c2D.cpp:45-99), evaluated warp-parallel:
+// cells [1, ncom) have every row's slice and its neighbour inside the
+// column; rows [min_v_all, max_v_all] stay inside it for every cell.
+__device__ __forceinline__ void cb_row_regimes(const Geom &g, const float *alphas, int n,
+                                               int lane, int &ncom, int &min_v_all,
+                                               int &max_v_all) {
+  const int nzm1 = g.nz - 1, mid = g.mid;
+  const float pzbz = g.pzbz, inv_dz = g.inv_dz;
+  ncom = 0;
+  min_v_all = mid;
+  max_v_all = mid - 1;
+  if (n < 2)
+    return;
+  int min_xy_all = n, max_xy_all = n;
+  const float dz0 = g.dz[0], dzl = g.dz[g.nv - 1];
+  bool got_lo = false, got_hi = false;
+  for (int m0 = 1; m0 < n && !(got_lo && got_hi); m0 += 32) {
+    const int m = m0 + lane;
+    int klo = 1, khi = nzm1 - 1;
+    if (m < n) {
+      const float av = __fmul_rn(alphas[m - 1], inv_dz);
+      klo = int(floorf(__fadd_rn(pzbz, __fmul_rn(av, dz0))));
+      khi = int(floorf(__fadd_rn(pzbz, __fmul_rn(av, dzl))));
+    }
+    if (!got_lo) {
+      const unsigned b = __ballot_sync(0xffffffffu, m < n && klo <= 0);
+      if (b) {
+        const int src = __ffs(b) - 1;
+        const int k = __shfl_sync(0xffffffffu, klo, src);
+        min_xy_all = (k == 0) ? m0 + src : 0;
+        got_lo = true;
+      }
+    }
+    if (!got_hi) {
+      const unsigned b = __ballot_sync(0xffffffffu, m < n && khi >= nzm1);
+      if (b) {
+        const int src = __ffs(b) - 1;
+        const int k = __shfl_sync(0xffffffffu, khi, src);
+        max_xy_all = (k == nzm1) ? m0 + src : 0;
+        got_hi = true;
+      }
+    }
+  }
+  ncom = min(min_xy_all, max_xy_all);
+  const float avl = __fmul_rn(alphas[n - 2], inv_dz);
+  for (int v0 = 0; v0 < mid; v0 += 32) {
+    const int v = v0 + lane;
+    const bool ok = v < mid && int(floorf(__fadd_rn(pzbz, __fmul_rn(avl, g.dz[v])))) > 0;
+    const unsigned b = __ballot_sync(0xffffffffu, ok);
+    if (b) {
+      min_v_all = v0 + __ffs(b) - 1;
+      break;
+    }
+  }
+  for (int v1 = g.nv - 1; v1 >= mid; v1 -= 32) {
+    const int v = v1 - lane;
+    const bool ok = v >= mid && int(floorf(__fadd_rn(pzbz, __fmul_rn(avl, g.dz[v])))) < nzm1;
+    const unsigned b = __ballot_sync(0xffffffffu, ok);
+    if (b) {
+      max_v_all = v1 - (__ffs(b) - 1);
+      break;
+    }
+  }
+}
+
 // RPL = detector rows per lane per pass (a pass covers 32 * RPL rows);
 // FULL: nv is a multiple of 32 * RPL (no idle rows).  nb volumes (one
 // after another) share each ray's walk and row regimes; EPI_STORE when
@@ -226,61 +291,8 @@ __global__ void __launch_bounds__(kFpWarps * 32)
       n = cb_walk(g, g.p1x[a], g.p1y[a], p2x, p2y, alphas, cells, cap);
     }
     __syncwarp();
-    // Row regimes (c2D.cpp:45-99), evaluated warp-parallel.
-    int ncom = 0, min_v_all = mid, max_v_all = mid - 1;
-    if (n >= 2) {
-      int min_xy_all = n, max_xy_all = n;
-      const float dz0 = g.dz[0], dzl = g.dz[g.nv - 1];
-      bool got_lo = false, got_hi = false;
-      for (int m0 = 1; m0 < n && !(got_lo && got_hi); m0 += 32) {
-        const int m = m0 + lane;
-        int klo = 1, khi = nzm1 - 1;
-        if (m < n) {
-          const float av = __fmul_rn(alphas[m - 1], inv_dz);
-          klo = int(floorf(__fadd_rn(pzbz, __fmul_rn(av, dz0))));
-          khi = int(floorf(__fadd_rn(pzbz, __fmul_rn(av, dzl))));
-        }
-        if (!got_lo) {
-          const unsigned b = __ballot_sync(0xffffffffu, m < n && klo <= 0);
-          if (b) {
-            const int src = __ffs(b) - 1;
-            const int k = __shfl_sync(0xffffffffu, klo, src);
-            min_xy_all = (k == 0) ? m0 + src : 0;
-            got_lo = true;
-          }
-        }
-        if (!got_hi) {
-          const unsigned b = __ballot_sync(0xffffffffu, m < n && khi >= nzm1);
-          if (b) {
-            const int src = __ffs(b) - 1;
-            const int k = __shfl_sync(0xffffffffu, khi, src);
-            max_xy_all = (k == nzm1) ? m0 + src : 0;
-            got_hi = true;
-          }
-        }
-      }
-      ncom = min(min_xy_all, max_xy_all);
-      const float avl = __fmul_rn(alphas[n - 2], inv_dz);
-      for (int v0 = 0; v0 < mid; v0 += 32) {
-        const int v = v0 + lane;
-        const bool ok = v < mid && int(floorf(__fadd_rn(pzbz, __fmul_rn(avl, g.dz[v])))) > 0;
-        const unsigned b = __ballot_sync(0xffffffffu, ok);
-        if (b) {
-          min_v_all = v0 + __ffs(b) - 1;
-          break;
-        }
-      }
-      for (int v1 = g.nv - 1; v1 >= mid; v1 -= 32) {
-        const int v = v1 - lane;
-        const bool ok =
-            v >= mid && int(floorf(__fadd_rn(pzbz, __fmul_rn(avl, g.dz[v])))) < nzm1;
-        const unsigned b = __ballot_sync(0xffffffffu, ok);
-        if (b) {
-          max_v_all = v1 - (__ffs(b) - 1);
-          break;
-        }
-      }
-    }
+    int ncom, min_v_all, max_v_all;
+    cb_row_regimes(g, alphas, n, lane, ncom, min_v_all, max_v_all);
     // Rows, RPL per lane per pass.  Cells [1, mfast) have every row inside
     // the slab (c2D.cpp:99-145); the rest take the edge rules (:146-190).
     const int mfast = min(ncom, n);
@@ -441,6 +453,168 @@ __global__ void __launch_bounds__(kFpWarps * 32)
   }
 }
 
+// ---- backward, ray-driven scatter (the transpose of cb_fp_kernel)
+//
+// One warp per ray (angle a, detector column h), as in the forward
+// projector, with the same walk.  The reference's back projector is not the
+// exact transpose of its forward projector: it drops rays parallel to an
+// axis and picks each row's slice rule from a band kept per voxel column
+// (c2D.cpp:657-750), where the forward projector keeps one per ray.  So
+// per (cell, row) this kernel takes the back projector's rule, from the
+// plan's column band table: slice k, neighbour and weights (mz - a0,
+// a1 - mz), and adds the row's value p = pix * d_conv to the two voxels.
+// Lanes hold consecutive rows, whose slices are non-decreasing in the lane,
+// so the warp sums the contributions per target voxel (a segmented
+// reduction over equal slice indices, as many doubling steps as the
+// longest run needs) and each run's first lane issues one float atomic add
+// per target.  The order of the
+// additions into a voxel is not fixed: the result equals the reference's
+// b2D to float rounding, not bit for bit (cb_bp_gather is that form).
+// `vol` must be zero on entry; PRE: `pix` is already scaled by d_conv.
+constexpr int kScatterRpl = 4; // rows per lane per pass of cb_bp_scatter
+template <int RPL, bool PRE>
+__global__ void __launch_bounds__(kFpWarps * 32)
+    cb_bp_scatter(Geom g, const float *__restrict__ pix, float *__restrict__ vol,
+                  const int2 *__restrict__ hrange, int cap) {
+  extern __shared__ unsigned char smem_raw[];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float *svz = reinterpret_cast<float *>(smem_raw);
+  float *alphas = svz + cb_vz_floats(g.nz) + size_t(wib) * 2 * cap;
+  int *cells = reinterpret_cast<int *>(alphas + cap);
+  for (int i = threadIdx.x; i <= g.nz; i += blockDim.x)
+    svz[i] = g.vz[i];
+  __syncthreads();
+  const int nrays = g.na * g.nh;
+  const int nz = g.nz, nzm1 = g.nz - 1, mid = g.mid;
+  const float pzbz = g.pzbz, pzbz1 = g.pzbz1, inv_dz = g.inv_dz;
+  for (int ray = blockIdx.x * kFpWarps + wib; ray < nrays; ray += gridDim.x * kFpWarps) {
+    const int a = ray / g.nh, h = ray - a * g.nh;
+    const int2 hr = hrange[a];
+    int n = 0;
+    if (h >= hr.x && h <= hr.y) {
+      const double c = g.cosA[a], s = g.sinA[a];
+      // the back projector takes no ray parallel to an axis
+      // (c2D.cpp:909-912), with its own differences
+      const double bdx = (g.cdx[a] - s * g.hpix[h]) - g.p1x[a];
+      const double bdy = (g.sdx[a] + c * g.hpix[h]) - g.p1y[a];
+      if (fabs(bdx) >= double(kEps) && fabs(bdy) >= double(kEps)) {
+        const double p2x = c * g.detx - s * g.hpix[h];
+        const double p2y = s * g.detx + c * g.hpix[h];
+        n = cb_walk(g, g.p1x[a], g.p1y[a], p2x, p2y, alphas, cells, cap);
+      }
+    }
+    __syncwarp();
+    const i64 rbase = i64(ray) * g.nv;
+    for (int vb = 0; n >= 2 && vb < g.nv; vb += 32 * RPL) {
+      float p[RPL], dzv[RPL], izv[RPL];
+      bool vok[RPL], below[RPL];
+#pragma unroll
+      for (int q = 0; q < RPL; q++) {
+        const int v = vb + q * 32 + lane;
+        vok[q] = v < g.nv;
+        below[q] = v < mid;
+        dzv[q] = vok[q] ? g.dz[v] : 0.0f;
+        izv[q] = vok[q] ? g.iz[v] : 0.0f;
+        const float y = vok[q] ? __ldg(pix + rbase + v) : 0.0f;
+        p[q] = (PRE || !vok[q]) ? y : __fmul_rn(y, g.dconv[i64(h) * g.nv + v]);
+      }
+      // the crossed column's band, loaded one cell ahead
+      int2 band_next = cells[0] >= 0 ? g.colband[cells[0]] : make_int2(0, 0);
+      for (int m = 1; m < n; m++) {
+        const int cell = cells[m - 1];
+        const int2 band = band_next;
+        if (m + 1 < n && cells[m] >= 0)
+          band_next = g.colband[cells[m]];
+        if (cell < 0)
+          continue;
+        const float a0 = alphas[m - 1], a1 = alphas[m];
+        const float av = __fmul_rn(a0, inv_dz);
+        float *col = vol + i64(cell) * nz;
+#pragma unroll
+        for (int q = 0; q < RPL; q++) {
+          const int v = vb + q * 32 + lane;
+          // the back projector's rule for this row (c2D.cpp:680-750): a
+          // band row feeds its slice k and the neighbour on the source's
+          // side (k - 1 below the source, k + 1 above), a row below the
+          // band k and k - 1, a row above it k and k + 1
+          int k = -1, kn = -1;
+          bool up = false;
+          float w1 = 0.0f, w2 = 0.0f;
+          if (vok[q]) {
+            if (v >= band.x && v < band.y) {
+              const int kk = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[q])));
+              const int kkn = below[q] ? kk - 1 : kk + 1;
+              if (unsigned(kk) <= unsigned(nzm1) && unsigned(kkn) <= unsigned(nzm1)) {
+                const float mz = fmin_ref(__fmul_rn(svz[below[q] ? kk : kk + 1], izv[q]), a1);
+                k = kk;
+                kn = kkn;
+                up = !below[q];
+                w1 = __fsub_rn(mz, a0);
+                w2 = __fsub_rn(a1, mz);
+              }
+            } else if (v < band.x) {
+              const int kk = int(__fadd_rn(pzbz1, __fmul_rn(av, dzv[q]))) - 1;
+              if (kk > 0 && kk <= nzm1) {
+                const float mz = fmin_ref(__fmul_rn(svz[kk], izv[q]), a1);
+                k = kk;
+                kn = kk - 1;
+                w1 = __fsub_rn(mz, a0);
+                w2 = __fsub_rn(a1, mz);
+              } else if (kk == 0) {
+                k = 0;
+                w1 = __fsub_rn(fmin_ref(__fmul_rn(svz[0], izv[q]), a1), a0);
+              }
+            } else {
+              const int kk = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[q])));
+              up = true;
+              if (kk < nzm1 && kk >= 0) {
+                const float mz = fmin_ref(__fmul_rn(svz[kk + 1], izv[q]), a1);
+                k = kk;
+                kn = kk + 1;
+                w1 = __fsub_rn(mz, a0);
+                w2 = __fsub_rn(a1, mz);
+              } else if (kk == nzm1) {
+                k = nzm1;
+                w1 = __fsub_rn(fmin_ref(__fmul_rn(svz[nz], izv[q]), a1), a0);
+              }
+            }
+          }
+          // per target voxel pair: runs of adjacent lanes with the same
+          // slice and neighbour side (slices are non-decreasing in the lane,
+          // so a voxel's rows are mostly one run; a split run only costs
+          // another atomic); rows that do not contribute get a key of their
+          // own.  Each run is summed in doubling steps that never
+          // cross the run's end, and its first lane adds the two sums.
+          const int key = k >= 0 ? 2 * k + (up ? 1 : 0) : -1 - lane;
+          const int next = __shfl_down_sync(0xffffffffu, key, 1);
+          const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+          const bool start = lane == 0 || prev != key;
+          const unsigned ends = __ballot_sync(0xffffffffu, lane == 31 || next != key);
+          const int run_end = lane + __ffs(ends >> lane) - 1;
+          // doubling steps until the warp's longest run is covered (rows
+          // usually change slice every row or two: none or one step)
+          const int longest = __reduce_max_sync(0xffffffffu, start ? run_end - lane + 1 : 1);
+          float s1 = __fmul_rn(p[q], w1), s2 = __fmul_rn(p[q], w2);
+          for (int d = 1; d < longest; d <<= 1) {
+            const float o1 = __shfl_down_sync(0xffffffffu, s1, d);
+            const float o2 = __shfl_down_sync(0xffffffffu, s2, d);
+            if (lane + d <= run_end) {
+              s1 = __fadd_rn(s1, o1);
+              s2 = __fadd_rn(s2, o2);
+            }
+          }
+          if (k >= 0 && start) {
+            atomicAdd(col + k, s1);
+            if (kn >= 0)
+              atomicAdd(col + kn, s2);
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // ---- backward
 constexpr int kBpThreads = 256;
 constexpr int kBpAngleChunk = 64;
@@ -492,6 +666,40 @@ __device__ void cb_column_rays(const Geom &g, int a, double x0, double xn, doubl
   }
 }
 
+// Band rows [lo, hi) of a ray entering a column at a0: rows whose slice and
+// its neighbour stay inside the column (c2D.cpp:664-668).
+__device__ __forceinline__ int cb_band_lo(const Geom &g, float a0) {
+  return int(ceilf(__fadd_rn(g.pzdeps, __fdiv_rn(g.z1, a0))));
+}
+__device__ __forceinline__ int cb_band_hi(const Geom &g, float a0) {
+  return int(floorf(__fadd_rn(g.pzdv, __fdiv_rn(g.znm, a0))));
+}
+
+// The back projector's band of every voxel column (c2D.cpp:657-676): the
+// rows inside the band of every ray that crosses the column.  One warp per
+// column, lanes over the angles; geometry only, built once per plan.
+constexpr int kBandWarps = 8;
+__global__ void __launch_bounds__(kBandWarps * 32) cb_column_band_kernel(Geom g, int2 *band) {
+  const int col = blockIdx.x * kBandWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (col >= g.nx * g.ny)
+    return; // the whole warp
+  const int i = col / g.ny, j = col - i * g.ny;
+  const double x0 = g.origin[0] + double(i) * g.size[0];
+  const double xn = g.origin[0] + double(i + 1) * g.size[0];
+  const double y0 = g.origin[1] + double(j) * g.size[1];
+  const double yn = g.origin[1] + double(j + 1) * g.size[1];
+  int lo = 0, hi = g.nv;
+  for (int a = lane; a < g.na; a += 32)
+    cb_column_rays(g, a, x0, xn, y0, yn, [&](int, float a0, float) {
+      lo = max(lo, cb_band_lo(g, a0));
+      hi = min(hi, cb_band_hi(g, a0));
+    });
+  lo = __reduce_max_sync(0xffffffffu, lo);
+  hi = __reduce_min_sync(0xffffffffu, hi);
+  if (lane == 0)
+    band[col] = make_int2(lo, hi);
+}
+
 template <int EPI>
 __global__ void __launch_bounds__(kBpThreads)
     cb_bp_kernel(Geom g, const float *__restrict__ pix, float *__restrict__ vol, Epi e,
@@ -512,20 +720,12 @@ __global__ void __launch_bounds__(kBpThreads)
   for (int z = threadIdx.x; z < g.nz; z += blockDim.x)
     acc[z] = 0.0f;
   if (threadIdx.x == 0) {
-    s_minv = 0;
-    s_maxv = g.nv;
+    // rows [min_v, max_v) stay inside the column for every ray
+    // (c2D.cpp:657-676), from the plan's table
+    const int2 b = g.colband[col];
+    s_minv = b.x;
+    s_maxv = b.y;
     s_ovf = 0;
-  }
-  __syncthreads();
-  // rows [min_v, max_v) stay inside the column for every ray (c2D.cpp:657-676)
-  for (int a = threadIdx.x; a < g.na; a += blockDim.x) {
-    int lo = 0, hi = g.nv;
-    cb_column_rays(g, a, x0, xn, y0, yn, [&](int, float a0, float) {
-      lo = max(lo, int(ceilf(__fadd_rn(g.pzdeps, __fdiv_rn(g.z1, a0)))));
-      hi = min(hi, int(floorf(__fadd_rn(g.pzdv, __fdiv_rn(g.znm, a0)))));
-    });
-    atomicMax(&s_minv, lo);
-    atomicMin(&s_maxv, hi);
   }
   __syncthreads();
   const int min_v = s_minv, max_v = s_maxv;
@@ -795,24 +995,16 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
     siz[t] = g.iz[t];
   }
   if (tid == 0) {
-    s_minv = 0;
-    s_maxv = nv;
+    // band limits over every ray of the column (c2D.cpp:657-676), from
+    // the plan's table
+    const int2 b = g.colband[col];
+    s_minv = b.x;
+    s_maxv = b.y;
     s_ovf = 0;
     s_box[0] = g.origin[0] + double(i) * g.size[0];
     s_box[1] = g.origin[0] + double(i + 1) * g.size[0];
     s_box[2] = g.origin[1] + double(j) * g.size[1];
     s_box[3] = g.origin[1] + double(j + 1) * g.size[1];
-  }
-  __syncthreads();
-  // band limits over every ray of the column (c2D.cpp:657-676)
-  for (int a = tid; a < g.na; a += blockDim.x) {
-    int lo = 0, hi = nv;
-    cb_column_rays(g, a, s_box[0], s_box[1], s_box[2], s_box[3], [&](int, float a0, float) {
-      lo = max(lo, int(ceilf(__fadd_rn(g.pzdeps, __fdiv_rn(g.z1, a0)))));
-      hi = min(hi, int(floorf(__fadd_rn(g.pzdv, __fdiv_rn(g.znm, a0)))));
-    });
-    atomicMax(&s_minv, lo);
-    atomicMin(&s_maxv, hi);
   }
   __syncthreads();
   const int min_v = s_minv, max_v = s_maxv;
@@ -1087,6 +1279,25 @@ size_t cb_fp_smem(const Geom &g) {
          sizeof(float);
 }
 
+int cb_backward_scatter(const Geom &g, const float *pix, float *vol, int pre,
+                        const int2 *hrange, int grid, cudaStream_t st) {
+  if (cudaMemsetAsync(vol, 0, size_t(g.nx) * g.ny * g.nz * sizeof(float), st) != cudaSuccess)
+    return 2;
+  const size_t smem = cb_fp_smem(g);
+  const int cap = g.nx + g.ny + 2;
+  if (pre)
+    cb_bp_scatter<kScatterRpl, true><<<grid, kFpWarps * 32, smem, st>>>(g, pix, vol, hrange, cap);
+  else
+    cb_bp_scatter<kScatterRpl, false><<<grid, kFpWarps * 32, smem, st>>>(g, pix, vol, hrange, cap);
+  return 0;
+}
+
+int cb_column_bands(const Geom &g, int2 *band, cudaStream_t st) {
+  const int ncol = g.nx * g.ny;
+  cb_column_band_kernel<<<(ncol + kBandWarps - 1) / kBandWarps, kBandWarps * 32, 0, st>>>(g, band);
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : 2;
+}
+
 namespace {
 // Rows per lane for nv rows: fewest idle lanes, then fewest passes.
 int cb_fp_rpl(int nv) {
@@ -1157,7 +1368,9 @@ int cb_prepare(const Geom &g) {
   (const void *)cb_fp_kernel<EPI_STORE, R, F>, (const void *)cb_fp_kernel<EPI_NORM, R, F>,  \
       (const void *)cb_fp_kernel<EPI_SIRT, R, F>, (const void *)cb_fp_kernel<EPI_MLEM, R, F>
   const void *fps[] = {CB_FP_ALL(4, false), CB_FP_ALL(8, false), CB_FP_ALL(12, false),
-                       CB_FP_ALL(4, true),  CB_FP_ALL(8, true),  CB_FP_ALL(12, true)};
+                       CB_FP_ALL(4, true),  CB_FP_ALL(8, true),  CB_FP_ALL(12, true),
+                       (const void *)cb_bp_scatter<kScatterRpl, false>,
+                       (const void *)cb_bp_scatter<kScatterRpl, true>};
 #undef CB_FP_ALL
   const void *bps[] = {(const void *)cb_bp_kernel<EPI_STORE>, (const void *)cb_bp_kernel<EPI_NORM>,
                        (const void *)cb_bp_kernel<EPI_SIRT>, (const void *)cb_bp_kernel<EPI_MLEM>};

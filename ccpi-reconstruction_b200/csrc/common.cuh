@@ -50,9 +50,13 @@ struct Geom {
   const float *vz;        // nz + 1: slice planes relative to src_z
   float inv_dz, pzbz, pzbz1, pzdv, z1, znm, pzdeps;
   int mid;                // first row above the source
+  // nx * ny: per voxel column the back projector's band rows [x, y) that
+  // stay inside the column for every ray crossing it (c2D.cpp:657-676)
+  const int2 *colband;
   // ---- launch shapes chosen by ccpi_plan_autotune (0: the built-in choice)
   int tune_vw;            // parallel back projector: slices per lane (4, 8, 16)
   int tune_rpl;           // cone forward projector: rows per lane (4, 8, 12)
+  int tune_scatter;       // cone back projector: 1 ray-driven scatter, 0 voxel gather
 };
 
 // Epilogue operands shared by the fused projector epilogues.

@@ -310,6 +310,12 @@ int plan_create(const ccpi_geometry *gi, ccpi_plan **out) {
       return 1;
     }
     ok = ok && cb_prepare(g) == 0;
+    if (ok) {
+      const std::vector<int2> none(size_t(g.nx) * g.ny, make_int2(0, 0));
+      int2 *band = upload(p, none);
+      ok = band && cb_column_bands(g, band, 0) == 0;
+      g.colband = band;
+    }
     p->fp_grid = int(std::min<i64>((i64(na) * nh + 3) / 4, 148 * 8));
     p->bp_parts = g.nx * g.ny;
   }
@@ -341,7 +347,28 @@ int backward(const ccpi_plan *p, const float *pix, float *vol, int mode, const E
              cudaStream_t st) {
   if (p->g.kind == CCPI_PARALLEL)
     return pb_backward(p->g, pix, vol, mode, e, p->err, st);
+  // the ray-driven scatter serves the plain and the norm forms (the CGLS
+  // family); the SIRT / MLEM epilogues need a voxel's finished sum and stay
+  // with the gather
+  if (p->g.tune_scatter && (mode == EPI_STORE || mode == EPI_NORM)) {
+    const int rc = cb_backward_scatter(p->g, pix, vol, e.pre, p->hrange, p->fp_grid, st);
+    if (mode == EPI_NORM)
+      k_sumsq_partials(vol, p->nvox, e.partials, sumsq_blocks(), st);
+    return rc;
+  }
   return cb_backward(p->g, pix, vol, mode, e, p->err, st);
+}
+
+int set_cone_backprojector(ccpi_plan *p, int scatter) {
+  if (p->g.kind != CCPI_CONE) {
+    set_error("ccpi_plan_set_cone_backprojector: not a cone-beam plan");
+    return 1;
+  }
+  p->g.tune_scatter = scatter ? 1 : 0;
+  // one FP64 partial sum per back-projector CTA (gather: one per column),
+  // or per block of the sum-of-squares pass after the scatter
+  p->bp_parts = scatter ? sumsq_blocks() : p->g.nx * p->g.ny;
+  return 0;
 }
 
 // ------------------------------------------------------------------ solvers
@@ -480,6 +507,11 @@ int backward_ones(const ccpi_plan *p, float *scratch_pix, float *vol, cudaStream
       return rc;
   }
   k_fill(scratch_pix, p->npix, 1.0f, st);
+  // cone: the SIRT / MLEM weights come from the deterministic gather
+  // whichever back projector the iterations use, so they equal the
+  // reference's bit for bit
+  if (p->g.kind == CCPI_CONE)
+    return cb_backward(p->g, scratch_pix, vol, EPI_STORE, e, p->err, st);
   return backward(p, scratch_pix, vol, EPI_STORE, e, st);
 }
 
@@ -1051,6 +1083,16 @@ int plan_autotune(ccpi_plan *p, cudaStream_t st, int *chosen) {
       }
     }
     p->g.tune_rpl = best_fp;
+    // back projector: the deterministic voxel gather or the ray-driven
+    // scatter, whichever is faster on this geometry
+    const float t_gather = timed([&] {
+      cb_backward(p->g, pix, vol, EPI_STORE, none, p->err, st);
+    });
+    const float t_scatter = timed([&] {
+      cb_backward_scatter(p->g, pix, vol, 0, p->hrange, p->fp_grid, st);
+    });
+    set_cone_backprojector(p, t_scatter < t_gather ? 1 : 0);
+    best_bp = p->g.tune_scatter;
   }
   if (rc == 0 && !cuda_ok(cudaStreamSynchronize(st), "autotune"))
     rc = 2;
@@ -1058,7 +1100,7 @@ int plan_autotune(ccpi_plan *p, cudaStream_t st, int *chosen) {
     rc = 16;
   if (chosen) {
     chosen[0] = p->g.kind == CCPI_PARALLEL ? p->fp_grid : p->g.tune_rpl;
-    chosen[1] = p->g.kind == CCPI_PARALLEL ? p->g.tune_vw : 0;
+    chosen[1] = p->g.kind == CCPI_PARALLEL ? p->g.tune_vw : p->g.tune_scatter;
   }
   if (e0)
     cudaEventDestroy(e0);

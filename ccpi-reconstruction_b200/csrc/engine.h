@@ -36,6 +36,9 @@ int backward(const ccpi_plan *p, const float *pix, float *vol, int mode, const E
 // be NULL) receives {forward grid or cone rows per lane, back projector
 // slices per lane or 0}.
 int plan_autotune(ccpi_plan *p, cudaStream_t st, int *chosen);
+// Cone plans: 1 selects the ray-driven scatter back projector for the plain
+// and norm forms, 0 the deterministic voxel gather (the default).
+int set_cone_backprojector(ccpi_plan *p, int scatter);
 size_t solve_workspace_bytes(const ccpi_plan *p, int alg, int niter);
 int solve(const ccpi_plan *p, int alg, const float *sino, float *x, int niter, double lambda,
           double *h_norms, int flags, void *ws, size_t ws_bytes, cudaStream_t st);

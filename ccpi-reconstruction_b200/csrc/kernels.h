@@ -14,6 +14,9 @@ int pb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi
                 int *err, cudaStream_t st);
 int pb_bp_tiles(const Geom &g);
 int cb_prepare(const Geom &g);
+// band[i * ny + j] = the back projector's band rows [x, y) of voxel column
+// (i, j) (c2D.cpp:657-676); the cone back projectors read it as g.colband
+int cb_column_bands(const Geom &g, int2 *band, cudaStream_t st);
 size_t cb_fp_smem(const Geom &g);
 size_t cb_bp_smem(const Geom &g);
 // nb / nbatch: that many volumes and sinograms one after another, one launch
@@ -22,6 +25,11 @@ int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi 
                const int2 *hrange, int grid, cudaStream_t st, int nb = 1);
 int cb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
                 int *err, cudaStream_t st, int nbatch = 1);
+// The ray-driven cone back projector (warp-aggregated atomics; order of the
+// additions not fixed): vol = A^T pix, EPI_STORE semantics; pre: pix is
+// already scaled by d_conv.  Launch shape of the forward projector.
+int cb_backward_scatter(const Geom &g, const float *pix, float *vol, int pre,
+                        const int2 *hrange, int grid, cudaStream_t st);
 // The cone back projector accepts a sinogram pre-scaled by d_conv (Epi::pre)
 // for this geometry; cb_prescale writes that scaled copy.
 bool cb_bp_takes_prescaled(const Geom &g);

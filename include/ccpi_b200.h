@@ -243,14 +243,27 @@ int ccpi_plan_create(const ccpi_geometry *geometry, ccpi_plan **plan);
 void ccpi_plan_destroy(ccpi_plan *plan);
 /* Time this plan's projector launch shapes on scratch data and keep the
  * fastest: the forward projector's grid (parallel beam) or rows per lane
- * (cone beam), and the parallel back projector's slices per lane.  No
- * counterpart in the reference (its block sizes are fixed).  Projections do
- * not depend on the choice; CGLS step scalars may change in the last FP64
- * bits (the number of partial sums follows the grid).  Call it after
- * ccpi_plan_create and before any solve or session on the plan.  chosen
- * (may be NULL) receives {grid or rows per lane, slices per lane or 0}.
- * Allocates and frees scratch of one volume and one sinogram. */
+ * (cone beam), the parallel back projector's slices per lane, and the cone
+ * back projector's form (ccpi_plan_set_cone_backprojector).  No
+ * counterpart in the reference (its block sizes are fixed).  Parallel
+ * projections do not depend on the choice; CGLS step scalars may change in
+ * the last FP64 bits (the number of partial sums follows the grid); the
+ * cone scatter form changes the back projection at float rounding.  Call it
+ * after ccpi_plan_create and before any solve or session on the plan.
+ * chosen (may be NULL) receives {grid or rows per lane, slices per lane (parallel)
+ * or 1 when the cone scatter was picked}.  Allocates and frees scratch of
+ * one volume and one sinogram. */
 int ccpi_plan_autotune(ccpi_plan *plan, void *stream, int chosen[2]);
+/* Cone beam: the form of the back projector used by ccpi_backward and the
+ * CGLS family (SIRT and MLEM always use the gather).  0 (the default): the
+ * voxel-driven gather, the reference's design (cone_beam::b2D,
+ * Core/src/c2D.cpp:948-1119) and equal to it bit for bit.  1: a ray-driven
+ * scatter over the forward projector's walk (c2D.cpp:193-467) that applies
+ * b2D's per-column row rules (c2D.cpp:657-750) and adds with
+ * warp-aggregated float atomics; equal to the reference to float rounding
+ * (the order of the additions is not fixed).
+ * ccpi_plan_autotune picks the faster for the plan's geometry. */
+int ccpi_plan_set_cone_backprojector(ccpi_plan *plan, int scatter);
 
 /* Measured ceiling of the projectors' gathers: GB/s at which the GPU reads
  * whole 1 KB columns at random offsets out of a working set of

@@ -238,7 +238,8 @@ def test_cgls_more_rows_than_one_projector_pass(cuda):
 def test_autotuned_plan_gives_the_same_results(kind, cuda):
     """ccpi_plan_autotune changes launch shapes only: projections and SIRT
     are bit-identical to the untuned plan, CGLS agrees to FP64 rounding of
-    its step scalars."""
+    its step scalars.  When it picks the cone scatter back projector, the
+    back projection and CGLS agree to the projector tolerance instead."""
     import torch
     from ccpi.reconstruction.device import cone_plan, parallel_plan
     mk = (lambda: parallel_plan((48, 48, 32), 60, 72)) if kind == "parallel" else \
@@ -246,11 +247,16 @@ def test_autotuned_plan_gives_the_same_results(kind, cuda):
     a, b = mk(), mk()
     chosen = b.autotune()
     assert chosen[0] > 0
+    scatter = kind == "cone" and chosen[1] == 1
     rng = np.random.default_rng(17)
     x = torch.from_numpy(rng.random(a.shape).astype(np.float32)).to(cuda)
     sa, sb = a.forward(x), b.forward(x)
     assert torch.equal(sa, sb)
-    assert torch.equal(a.backward(sa), b.backward(sb))
+    ba, bb = a.backward(sa), b.backward(sb)
+    if scatter:
+        assert max_rel(bb.cpu().numpy(), ba.cpu().numpy()) <= 1e-5
+    else:
+        assert torch.equal(ba, bb)
     for alg, exact in ((1, True), (0, False)):
         xa = torch.zeros(a.shape, device=cuda)
         xb = torch.zeros(b.shape, device=cuda)
@@ -259,7 +265,7 @@ def test_autotuned_plan_gives_the_same_results(kind, cuda):
         if exact:
             assert torch.equal(xa, xb)
         else:
-            assert rel_l2(xb.cpu().numpy(), xa.cpu().numpy()) <= 1e-6
+            assert rel_l2(xb.cpu().numpy(), xa.cpu().numpy()) <= (1e-5 if scatter else 1e-6)
 
 
 def test_sirt_full_size_slices_equal_single_slice_solves(cuda):
