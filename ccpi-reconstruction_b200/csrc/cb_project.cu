@@ -465,15 +465,15 @@ __global__ void __launch_bounds__(kFpWarps * 32)
 // a1 - mz), and adds the row's value p = pix * d_conv to the two voxels.
 // Lanes hold consecutive rows, whose slices are non-decreasing in the lane,
 // so the warp sums the contributions per target voxel (a segmented
-// reduction over equal slice indices, as many doubling steps as the
-// longest run needs) and each run's first lane issues one float atomic add
-// per target.  The order of the
+// reduction over equal slice indices, three doubling steps unless a run
+// is longer than 8 lanes) and each run's first lane issues one float atomic
+// add per target.  The order of the
 // additions into a voxel is not fixed: the result equals the reference's
 // b2D to float rounding, not bit for bit (cb_bp_gather is that form).
 // `vol` must be zero on entry; PRE: `pix` is already scaled by d_conv.
 constexpr int kScatterRpl = 4; // rows per lane per pass of cb_bp_scatter
 template <int RPL, bool PRE>
-__global__ void __launch_bounds__(kFpWarps * 32)
+__global__ void __launch_bounds__(kFpWarps * 32, 8)
     cb_bp_scatter(Geom g, const float *__restrict__ pix, float *__restrict__ vol,
                   const int2 *__restrict__ hrange, int cap) {
   extern __shared__ unsigned char smem_raw[];
@@ -530,6 +530,9 @@ __global__ void __launch_bounds__(kFpWarps * 32)
         const float a0 = alphas[m - 1], a1 = alphas[m];
         const float av = __fmul_rn(a0, inv_dz);
         float *col = vol + i64(cell) * nz;
+        int kq[RPL], knq[RPL], endq[RPL];
+        float s1[RPL], s2[RPL];
+        bool startq[RPL], longq = false;
 #pragma unroll
         for (int q = 0; q < RPL; q++) {
           const int v = vb + q * 32 + lane;
@@ -583,30 +586,47 @@ __global__ void __launch_bounds__(kFpWarps * 32)
           // slice and neighbour side (slices are non-decreasing in the lane,
           // so a voxel's rows are mostly one run; a split run only costs
           // another atomic); rows that do not contribute get a key of their
-          // own.  Each run is summed in doubling steps that never
-          // cross the run's end, and its first lane adds the two sums.
+          // own
           const int key = k >= 0 ? 2 * k + (up ? 1 : 0) : -1 - lane;
           const int next = __shfl_down_sync(0xffffffffu, key, 1);
           const int prev = __shfl_up_sync(0xffffffffu, key, 1);
-          const bool start = lane == 0 || prev != key;
           const unsigned ends = __ballot_sync(0xffffffffu, lane == 31 || next != key);
-          const int run_end = lane + __ffs(ends >> lane) - 1;
-          // doubling steps until the warp's longest run is covered (rows
-          // usually change slice every row or two: none or one step)
-          const int longest = __reduce_max_sync(0xffffffffu, start ? run_end - lane + 1 : 1);
-          float s1 = __fmul_rn(p[q], w1), s2 = __fmul_rn(p[q], w2);
-          for (int d = 1; d < longest; d <<= 1) {
-            const float o1 = __shfl_down_sync(0xffffffffu, s1, d);
-            const float o2 = __shfl_down_sync(0xffffffffu, s2, d);
-            if (lane + d <= run_end) {
-              s1 = __fadd_rn(s1, o1);
-              s2 = __fadd_rn(s2, o2);
+          kq[q] = k;
+          knq[q] = kn;
+          startq[q] = k >= 0 && (lane == 0 || prev != key);
+          endq[q] = lane + __ffs(ends >> lane) - 1;
+          longq |= endq[q] - lane >= 8;
+          s1[q] = __fmul_rn(p[q], w1);
+          s2[q] = __fmul_rn(p[q], w2);
+        }
+        // each run summed in doubling steps that never cross its end, the
+        // RPL row groups side by side; three steps cover runs of up to 8
+        // lanes, the usual case (a slice takes a few rows), five any run
+        auto step = [&](int d) {
+#pragma unroll
+          for (int q = 0; q < RPL; q++) {
+            const float o1 = __shfl_down_sync(0xffffffffu, s1[q], d);
+            const float o2 = __shfl_down_sync(0xffffffffu, s2[q], d);
+            if (lane + d <= endq[q]) {
+              s1[q] = __fadd_rn(s1[q], o1);
+              s2[q] = __fadd_rn(s2[q], o2);
             }
           }
-          if (k >= 0 && start) {
-            atomicAdd(col + k, s1);
-            if (kn >= 0)
-              atomicAdd(col + kn, s2);
+        };
+        step(1);
+        step(2);
+        step(4);
+        if (__any_sync(0xffffffffu, longq)) {
+          step(8);
+          step(16);
+        }
+        // each run's first lane adds the two sums
+#pragma unroll
+        for (int q = 0; q < RPL; q++) {
+          if (startq[q]) {
+            atomicAdd(col + kq[q], s1[q]);
+            if (knq[q] >= 0)
+              atomicAdd(col + knq[q], s2[q]);
           }
         }
       }
