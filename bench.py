@@ -79,6 +79,9 @@ def parse():
     ap.add_argument("--cone-n", type=int, default=CN,
                     help="cone grid edge (512: the CGLS workload; 256: 360 angles onto a 384^2 "
                          "detector at 1.6 mm, 2 mm voxels, for profiler captures)")
+    ap.add_argument("--cone-bp", default="auto", choices=["auto", "gather", "scatter"],
+                    help="cone back projector: auto (ccpi_plan_autotune times both, outside "
+                         "the timed region), the voxel gather or the ray-driven scatter")
     args = ap.parse_args()
     if args.small:
         g = globals()
@@ -91,7 +94,8 @@ def load_traffic(kernel):
     """DRAM bytes per launch of `kernel` on the full-size workload, from one
     ncu capture of the same command (1-pass metrics), kept in profiles/."""
     name = {"pb_fp": "pb_traffic_768x768x256.json", "pb_bp": "pb_traffic_768x768x256.json",
-            "cb_bp": "cb_traffic_512cube.json", "cb_fp": "cb_traffic_512cube.json"}.get(kernel)
+            "cb_bp_gather": "cb_traffic_512cube.json", "cb_bp_scatter": "cb_traffic_512cube.json",
+            "cb_fp": "cb_traffic_512cube.json"}.get(kernel)
     if name is None or (kernel.startswith("pb") and globals().get("NH") != 768):
         return None
     try:
@@ -99,6 +103,20 @@ def load_traffic(kernel):
             return float(json.load(f)["kernels"][kernel]["dram_bytes_per_launch"])
     except Exception:
         return None
+
+
+def pick_cone_bp(plan, choice):
+    """Set the cone plan's back projector as --cone-bp asks; returns
+    (kernel name, seconds the autotuner took or 0)."""
+    t = 0.0
+    if choice == "auto":
+        t0 = time.perf_counter()
+        scatter = plan.autotune()[1] == 1
+        t = time.perf_counter() - t0
+    else:
+        scatter = choice == "scatter"
+        plan.set_cone_backprojector(1 if scatter else 0)
+    return ("cb_bp_scatter" if scatter else "cb_bp_gather"), t
 
 
 def load_peaks():
@@ -432,6 +450,7 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
     n, vs, na, nd, px = cone_geometry(args.cone_n)
     full = n == CN
     plan = cone_plan(n, vs, na, nd, px, CS2O, CO2D)
+    bp_kernel, t_tune = pick_cone_bp(plan, args.cone_bp)
     vol_np = ellipsoid_phantom(n, 40, (10.0 * n / CN, 120.0 * n / CN), seed=3 + rank)
     clean = plan.forward(torch.from_numpy(vol_np).to(dev))
     mu = 3.0 / float(clean.max())
@@ -510,7 +529,7 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
     peak, peak_kind = load_peaks()
     bp_bytes = 4.0 * (V + P)
     it_bytes = 4.0 * (7 * V + 4 * P)
-    traffic = load_traffic("cb_bp")
+    traffic = load_traffic(bp_kernel)
     value = world * args.steps / t_cgls
     t_it = t_cgls / args.steps
     return {
@@ -531,7 +550,7 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
         "plain_iter_per_s": (1.0 / plain) if plain else None,
         "batched_over_plain": (plain / t_it) if plain else None,
         "plain_form": "host-driven iterations, step scalars read back each iteration",
-        "roofline": {"bound": "hbm", "kernel": "cb_bp_gather (back projection)",
+        "roofline": {"bound": "hbm", "kernel": bp_kernel + " (back projection)",
                      "achieved": bp_bytes / t_bp / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": bp_bytes / t_bp / 1e9 / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bp_bytes,
@@ -551,8 +570,11 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
                         "sinogram and volume; plan, upload, set-up and download inside"
                         % args.steps},
         # per iteration: forward, alpha, residual update, d_conv pre-scale,
-        # back projection, beta, x/d update
-        "gpu_launches": 7 * args.steps,
+        # back projection, beta, x/d update; the scatter's norm form adds a
+        # sum-of-squares pass (its zero fill is a memset node)
+        "gpu_launches": (8 if bp_kernel == "cb_bp_scatter" else 7) * args.steps,
+        "back_projector": {"kernel": bp_kernel, "choice": args.cone_bp,
+                           "autotune_seconds": t_tune},
         "clocks": clk,
         "residual_norms": [float(n_) for n_ in norms[-3:]],
         "fp64_oracle": fp64,
@@ -969,6 +991,7 @@ def run_cone_projectors(args):
     torch.cuda.set_device(dev)
     n, vs, na, nd, px = cone_geometry(args.cone_n)
     plan = cone_plan(n, vs, na, nd, px, CS2O, CO2D)
+    bp_kernel, _ = pick_cone_bp(plan, args.cone_bp)
     vol = torch.from_numpy(ellipsoid_phantom(n, 40, (10.0 * n / CN, 120.0 * n / CN), seed=3)).to(dev)
     sino = plan.forward(vol)
     out = torch.empty_like(vol)
@@ -984,7 +1007,7 @@ def run_cone_projectors(args):
         P / t_bp, "rays/s", t_fp + t_bp, {"grid": [n] * 3, "angles": na, "detector": [nd, nd]},
         fp_ms=1000 * t_fp, bp_ms=1000 * t_bp,
         projector_rays_per_s={"forward": P / t_fp, "backward": P / t_bp},
-        roofline={"bound": "hbm", "kernel": "cb_bp_gather", "achieved": 4.0 * (V + P) / t_bp / 1e9,
+        roofline={"bound": "hbm", "kernel": bp_kernel, "achieved": 4.0 * (V + P) / t_bp / 1e9,
                   "peak": peak, "unit": "GB/s", "frac": 4.0 * (V + P) / t_bp / 1e9 / peak,
                   "peak_kind": peak_kind},
         gpu_launches=2 * args.steps)))

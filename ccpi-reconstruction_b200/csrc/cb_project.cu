@@ -261,10 +261,11 @@ __device__ __forceinline__ void cb_row_regimes(const Geom &g, const float *alpha
 }
 
 // RPL = detector rows per lane per pass (a pass covers 32 * RPL rows);
-// FULL: nv is a multiple of 32 * RPL (no idle rows).  nb volumes (one
-// after another) share each ray's walk and row regimes; EPI_STORE when
-// nb > 1.
-template <int EPI, int RPL, bool FULL>
+// FULL: nv is a multiple of 32 * RPL (no idle rows).  BATCH: nb volumes
+// (one after another) share each ray's walk and row regimes (EPI_STORE
+// only).  Without it the item loop runs once and compiles away: a run-time
+// loop costs the single-volume form 10 % at 512^3.
+template <int EPI, int RPL, bool FULL, bool BATCH>
 __global__ void __launch_bounds__(kFpWarps * 32)
     cb_fp_kernel(Geom g, const float *__restrict__ vol0, float *__restrict__ pix0, Epi e,
                  const int2 *__restrict__ hrange, int cap, int nb) {
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(kFpWarps * 32)
     // Rows, RPL per lane per pass.  Cells [1, mfast) have every row inside
     // the slab (c2D.cpp:99-145); the rest take the edge rules (:146-190).
     const int mfast = min(ncom, n);
-    for (int b = 0; b < nb; b++) {
+    for (int b = 0; b < (BATCH ? nb : 1); b++) {
     // batch item b: its volume and its sinogram
     const float *__restrict__ vol = vol0 + i64(b) * g.nx * g.ny * g.nz;
     float *__restrict__ pix = pix0 + i64(b) * g.na * g.nh * g.nv;
@@ -981,7 +982,9 @@ __device__ __forceinline__ void cb_ga_mark(int *f, int kp, int k, int v, int nz)
 // PRE: the sinogram is already scaled by d_conv (the reference's dpixels,
 // c2D.cpp:1096-1117, formed by the producer of the back projector's input),
 // so a staged row is one load and no multiply.  ST rays per stage.
-template <int EPI, int NZT, int RMAX, bool PRE, int ST>
+// BATCH: nbatch sinograms (EPI_STORE only); without it the item loop runs
+// once and compiles away.
+template <int EPI, int NZT, int RMAX, bool PRE, int ST, bool BATCH>
 __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
     cb_bp_gather(Geom g, const float *__restrict__ pix0, float *__restrict__ vol0, Epi e,
                  int *err, int nbatch) {
@@ -1047,7 +1050,7 @@ __global__ void __launch_bounds__(kGaThreads, NZT == 1 ? 4 : (NZT == 2 ? 3 : 2))
   const float sd_first = nb > 0 ? sdz[min_v] : 0.0f, sd_last = nb > 0 ? sdz[max_v - 1] : 0.0f;
   double ssq = 0.0;
   // nbatch sinograms (one after another) share the column's band limits
-  for (int bi = 0; bi < nbatch; bi++) {
+  for (int bi = 0; bi < (BATCH ? nbatch : 1); bi++) {
   const float *__restrict__ pix = pix0 + i64(bi) * g.na * g.nh * nv;
   float *__restrict__ vol = vol0 + i64(bi) * g.nx * g.ny * nz;
   float acc[NZT];
@@ -1345,14 +1348,25 @@ void launch_cb_fp(const Geom &g, const float *vol, float *pix, const Epi &e, con
   const int r = (g.tune_rpl == 4 || g.tune_rpl == 8 || g.tune_rpl == 12) ? g.tune_rpl
                                                                           : cb_fp_rpl(g.nv);
   const bool full = g.nv % (32 * r) == 0;
-#define CB_FP_GO(R, F)                                                                     \
-  cb_fp_kernel<EPI, R, F><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap, nb)
+#define CB_FP_GO(R, F, B)                                                                  \
+  cb_fp_kernel<EPI, R, F, B><<<grid, kFpWarps * 32, smem, st>>>(g, vol, pix, e, hrange, cap, nb)
+  if constexpr (EPI == EPI_STORE) {
+    if (nb > 1) {
+      if (r == 12)
+        full ? CB_FP_GO(12, true, true) : CB_FP_GO(12, false, true);
+      else if (r == 8)
+        full ? CB_FP_GO(8, true, true) : CB_FP_GO(8, false, true);
+      else
+        full ? CB_FP_GO(4, true, true) : CB_FP_GO(4, false, true);
+      return;
+    }
+  }
   if (r == 12)
-    full ? CB_FP_GO(12, true) : CB_FP_GO(12, false);
+    full ? CB_FP_GO(12, true, false) : CB_FP_GO(12, false, false);
   else if (r == 8)
-    full ? CB_FP_GO(8, true) : CB_FP_GO(8, false);
+    full ? CB_FP_GO(8, true, false) : CB_FP_GO(8, false, false);
   else
-    full ? CB_FP_GO(4, true) : CB_FP_GO(4, false);
+    full ? CB_FP_GO(4, true, false) : CB_FP_GO(4, false, false);
 #undef CB_FP_GO
 }
 } // namespace
@@ -1385,8 +1399,11 @@ int cb_prepare(const Geom &g) {
   const int ga = int(cb_bp_gather_smem(g));
   cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
 #define CB_FP_ALL(R, F)                                                                    \
-  (const void *)cb_fp_kernel<EPI_STORE, R, F>, (const void *)cb_fp_kernel<EPI_NORM, R, F>,  \
-      (const void *)cb_fp_kernel<EPI_SIRT, R, F>, (const void *)cb_fp_kernel<EPI_MLEM, R, F>
+  (const void *)cb_fp_kernel<EPI_STORE, R, F, false>,                                       \
+      (const void *)cb_fp_kernel<EPI_NORM, R, F, false>,                                    \
+      (const void *)cb_fp_kernel<EPI_SIRT, R, F, false>,                                    \
+      (const void *)cb_fp_kernel<EPI_MLEM, R, F, false>,                                    \
+      (const void *)cb_fp_kernel<EPI_STORE, R, F, true>
   const void *fps[] = {CB_FP_ALL(4, false), CB_FP_ALL(8, false), CB_FP_ALL(12, false),
                        CB_FP_ALL(4, true),  CB_FP_ALL(8, true),  CB_FP_ALL(12, true),
                        (const void *)cb_bp_scatter<kScatterRpl, false>,
@@ -1402,14 +1419,16 @@ int cb_prepare(const Geom &g) {
       e2 = cudaErrorInvalidValue;
   if (cb_bp_gather_nzt(g)) {
 #define CB_GA_EPI(Z, R)                                                                    \
-  (const void *)cb_bp_gather<EPI_STORE, Z, R, false, CB_GA_STAGE>,                          \
-      (const void *)cb_bp_gather<EPI_NORM, Z, R, false, CB_GA_STAGE>,                       \
-      (const void *)cb_bp_gather<EPI_SIRT, Z, R, false, CB_GA_STAGE>,                       \
-      (const void *)cb_bp_gather<EPI_MLEM, Z, R, false, CB_GA_STAGE>,                       \
-      (const void *)cb_bp_gather<EPI_STORE, Z, R, true, CB_GA_STAGE_PRE>,                   \
-      (const void *)cb_bp_gather<EPI_NORM, Z, R, true, CB_GA_STAGE_PRE>,                    \
-      (const void *)cb_bp_gather<EPI_SIRT, Z, R, true, CB_GA_STAGE_PRE>,                    \
-      (const void *)cb_bp_gather<EPI_MLEM, Z, R, true, CB_GA_STAGE_PRE>
+  (const void *)cb_bp_gather<EPI_STORE, Z, R, false, CB_GA_STAGE, false>,                   \
+      (const void *)cb_bp_gather<EPI_NORM, Z, R, false, CB_GA_STAGE, false>,                \
+      (const void *)cb_bp_gather<EPI_SIRT, Z, R, false, CB_GA_STAGE, false>,                \
+      (const void *)cb_bp_gather<EPI_MLEM, Z, R, false, CB_GA_STAGE, false>,                \
+      (const void *)cb_bp_gather<EPI_STORE, Z, R, true, CB_GA_STAGE_PRE, false>,            \
+      (const void *)cb_bp_gather<EPI_NORM, Z, R, true, CB_GA_STAGE_PRE, false>,             \
+      (const void *)cb_bp_gather<EPI_SIRT, Z, R, true, CB_GA_STAGE_PRE, false>,             \
+      (const void *)cb_bp_gather<EPI_MLEM, Z, R, true, CB_GA_STAGE_PRE, false>,             \
+      (const void *)cb_bp_gather<EPI_STORE, Z, R, false, CB_GA_STAGE, true>,                \
+      (const void *)cb_bp_gather<EPI_STORE, Z, R, true, CB_GA_STAGE_PRE, true>
 #define CB_GA_ALL(Z) CB_GA_EPI(Z, 1), CB_GA_EPI(Z, 2), CB_GA_EPI(Z, 3), CB_GA_EPI(Z, 4)
     const void *gas[] = {CB_GA_ALL(1), CB_GA_ALL(2), CB_GA_ALL(4)};
 #undef CB_GA_EPI
@@ -1458,18 +1477,32 @@ void launch_cb_ga(const Geom &g, int nzt, int rmax, const float *pix, float *vol
                   int *err, cudaStream_t st, int nbatch) {
   const int ncol = g.nx * g.ny;
   const size_t gsm = cb_bp_gather_smem(g);
-#define CB_GA_GO(Z)                                                                        \
-  (rmax == 1   ? cb_bp_gather<EPI, Z, 1, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err, nbatch) \
-   : rmax == 2 ? cb_bp_gather<EPI, Z, 2, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err, nbatch) \
-   : rmax == 3 ? cb_bp_gather<EPI, Z, 3, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err, nbatch) \
-               : cb_bp_gather<EPI, Z, 4, PRE, ST><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err, nbatch))
+#define CB_GA_ONE(Z, R, B)                                                                 \
+  cb_bp_gather<EPI, Z, R, PRE, ST, B><<<ncol, kGaThreads, gsm, st>>>(g, pix, vol, e, err, nbatch)
+#define CB_GA_GO(Z, B)                                                                     \
+  (rmax == 1   ? CB_GA_ONE(Z, 1, B)                                                         \
+   : rmax == 2 ? CB_GA_ONE(Z, 2, B)                                                         \
+   : rmax == 3 ? CB_GA_ONE(Z, 3, B)                                                         \
+               : CB_GA_ONE(Z, 4, B))
+  if constexpr (EPI == EPI_STORE) {
+    if (nbatch > 1) {
+      if (nzt == 1)
+        CB_GA_GO(1, true);
+      else if (nzt == 2)
+        CB_GA_GO(2, true);
+      else
+        CB_GA_GO(4, true);
+      return;
+    }
+  }
   if (nzt == 1)
-    CB_GA_GO(1);
+    CB_GA_GO(1, false);
   else if (nzt == 2)
-    CB_GA_GO(2);
+    CB_GA_GO(2, false);
   else
-    CB_GA_GO(4);
+    CB_GA_GO(4, false);
 #undef CB_GA_GO
+#undef CB_GA_ONE
 }
 
 template <int EPI>
