@@ -486,12 +486,16 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
 
     # ---- plain: host-driven iterations (each iteration's launches from the
     # host, step scalars read back every iteration)
+    # (a session: set-up and workspace outside the timed region, W warm-up
+    # iterations, then K iterations between CUDA events, as for `value`)
     plain = None
     if not args.no_plain:
         xp = torch.zeros(plan.shape, device=dev)
-        t2 = cuda_time(torch, lambda: plan.solve(N.CGLS, sino, xp, 2, plain=True))
-        t1 = cuda_time(torch, lambda: plan.solve(N.CGLS, sino, xp, 1, plain=True))
-        plain = max(t2 - t1, 1e-9)
+        ps = Session(plan, N.CGLS, sino, xp, args.warmup + args.steps, plain=True)
+        ps.run(args.warmup)
+        plain = cuda_time(torch, lambda: ps.run(args.steps)) / args.steps
+        ps.finish()
+        ps.close()
         del xp
 
     # ---- e2e: ccpi_reconstruct with pinned host buffers (upload, plan, set-up,

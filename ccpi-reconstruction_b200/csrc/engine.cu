@@ -1084,12 +1084,16 @@ int plan_autotune(ccpi_plan *p, cudaStream_t st, int *chosen) {
     }
     p->g.tune_rpl = best_fp;
     // back projector: the deterministic voxel gather or the ray-driven
-    // scatter, whichever is faster on this geometry
+    // scatter, whichever is faster on this geometry, each timed in the
+    // form the CGLS iterations run (on a sinogram pre-scaled by d_conv
+    // where the gather takes one; the scratch values do not matter)
+    Epi pre{};
+    pre.pre = cb_bp_takes_prescaled(p->g) ? 1 : 0;
     const float t_gather = timed([&] {
-      cb_backward(p->g, pix, vol, EPI_STORE, none, p->err, st);
+      cb_backward(p->g, pix, vol, EPI_STORE, pre, p->err, st);
     });
     const float t_scatter = timed([&] {
-      cb_backward_scatter(p->g, pix, vol, 0, p->hrange, p->fp_grid, st);
+      cb_backward_scatter(p->g, pix, vol, pre.pre, p->hrange, p->fp_grid, st);
     });
     set_cone_backprojector(p, t_scatter < t_gather ? 1 : 0);
     best_bp = p->g.tune_scatter;

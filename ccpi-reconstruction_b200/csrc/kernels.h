@@ -25,9 +25,10 @@ int cb_forward(const Geom &g, const float *vol, float *pix, int mode, const Epi 
                const int2 *hrange, int grid, cudaStream_t st, int nb = 1);
 int cb_backward(const Geom &g, const float *pix, float *vol, int mode, const Epi &e,
                 int *err, cudaStream_t st, int nbatch = 1);
-// The ray-driven cone back projector (warp-aggregated atomics; order of the
-// additions not fixed): vol = A^T pix, EPI_STORE semantics; pre: pix is
-// already scaled by d_conv.  Launch shape of the forward projector.
+// The ray-driven cone back projector (each lane sums runs of its rows in
+// registers and adds them with float atomics; order of the additions not
+// fixed): vol = A^T pix, EPI_STORE semantics; pre: pix is already scaled
+// by d_conv.  Launch shape of the forward projector.
 int cb_backward_scatter(const Geom &g, const float *pix, float *vol, int pre,
                         const int2 *hrange, int grid, cudaStream_t st);
 // The cone back projector accepts a sinogram pre-scaled by d_conv (Epi::pre)

@@ -244,7 +244,8 @@ void ccpi_plan_destroy(ccpi_plan *plan);
 /* Time this plan's projector launch shapes on scratch data and keep the
  * fastest: the forward projector's grid (parallel beam) or rows per lane
  * (cone beam), the parallel back projector's slices per lane, and the cone
- * back projector's form (ccpi_plan_set_cone_backprojector).  No
+ * back projector's form (ccpi_plan_set_cone_backprojector; both forms timed
+ * on a sinogram pre-scaled by d_conv, as the CGLS iterations run them).  No
  * counterpart in the reference (its block sizes are fixed).  Parallel
  * projections do not depend on the choice; CGLS step scalars may change in
  * the last FP64 bits (the number of partial sums follows the grid); the
@@ -259,9 +260,10 @@ int ccpi_plan_autotune(ccpi_plan *plan, void *stream, int chosen[2]);
  * voxel-driven gather, the reference's design (cone_beam::b2D,
  * Core/src/c2D.cpp:948-1119) and equal to it bit for bit.  1: a ray-driven
  * scatter over the forward projector's walk (c2D.cpp:193-467) that applies
- * b2D's per-column row rules (c2D.cpp:657-750) and adds with
- * warp-aggregated float atomics; equal to the reference to float rounding
- * (the order of the additions is not fixed).
+ * b2D's per-column row rules (c2D.cpp:657-750); each lane sums runs of its
+ * consecutive detector rows that feed the same voxels in registers and adds
+ * them with float atomics.  Equal to the reference to float rounding (the
+ * order of the additions is not fixed).
  * ccpi_plan_autotune picks the faster for the plan's geometry. */
 int ccpi_plan_set_cone_backprojector(ccpi_plan *plan, int scatter);
 
