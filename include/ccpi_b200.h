@@ -291,7 +291,9 @@ int ccpi_backward(const ccpi_plan *plan, const float *d_sino, float *d_volume,
  * of volumes under torch autograd.  Cone beam runs one launch per
  * direction, the batch sharing each ray's xy walk and each column's ray
  * list (f2D / b2D, Core/src/c2D.cpp:469-625, :948-1119, called once per
- * item in the reference); parallel beam one launch per item.  Every item
+ * item in the reference); parallel beam one launch per item.  The cone
+ * batch back projection is the voxel gather whichever form
+ * ccpi_plan_set_cone_backprojector chose for single calls.  Every item
  * must start on a 16-byte boundary. */
 int ccpi_forward_batch(const ccpi_plan *plan, int n, const float *d_volumes, float *d_sinos,
                        void *stream);
