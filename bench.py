@@ -509,11 +509,15 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
     del sino, x
     torch.cuda.empty_cache()
 
+    # the call a user makes, with the back projector the autotuner chose for
+    # the device plan (ccpi_reconstruct_flags, CCPI_RECON_CONE_SCATTER)
+    e2e_form = "scatter" if bp_kernel == "cb_bp_scatter" else "gather"
+
     def e2e():
         out = CA.reconstruct_explicit("cgls", geo["source"], geo["detector_x"], geo["h_pixels"],
                                       geo["v_pixels"], geo["angles"], host_s.numpy(),
                                       geo["grid_offset"], geo["voxel_size"], geo["shape"],
-                                      args.steps)
+                                      args.steps, backprojector=e2e_form)
         host_x.numpy()[...] = out
     barrier()
     t0 = time.perf_counter()
@@ -570,9 +574,9 @@ def cone_line(args, torch, dev, world, rank, barrier, max_over_ranks):
         "e2e": {"value": world * args.steps / t_e2e, "unit": "iter/s",
                 "h2d_bytes_per_step": 4.0 * P / args.steps,
                 "d2h_bytes_per_step": 4.0 * V / args.steps,
-                "call": "ccpi_reconstruct(cone geometry, CGLS, %d iterations), pinned host "
-                        "sinogram and volume; plan, upload, set-up and download inside"
-                        % args.steps},
+                "call": "ccpi_reconstruct_flags(cone geometry, CGLS, %d iterations, %s back "
+                        "projector), pinned host sinogram and volume; plan, upload, set-up and "
+                        "download inside" % (args.steps, e2e_form)},
         # per iteration: forward, alpha, residual update, d_conv pre-scale,
         # back projection, beta, x/d update; the scatter's norm form adds a
         # sum-of-squares pass (its zero fill is a memset node)

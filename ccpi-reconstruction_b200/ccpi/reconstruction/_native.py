@@ -17,6 +17,7 @@ LIB_PATH = os.environ.get("CCPI_B200_LIB", os.path.join(_PKG_ROOT, "libccpi_b200
 CGLS, SIRT, MLEM, CGLS_TIKHONOV, CGLS_TV = 0, 1, 2, 3, 4
 PARALLEL, CONE = 0, 1
 SOLVE_PLAIN = 1
+RECON_CONE_SCATTER = 1
 
 _c_int, _c_dbl, _vp, _sz = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_size_t
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -72,6 +73,8 @@ def _load():
         [_c_dbl] * 5 + [_c_int, _c_int, _c_int, _c_dbl, _vp, _f32p]
     lib.ccpi_cb_create_sinogram.argtypes = [P(Geometry), _f32p, _f32p]
     lib.ccpi_reconstruct.argtypes = [P(Geometry), _c_int, _vp, _c_int, _c_dbl, _vp, _vp]
+    lib.ccpi_reconstruct_flags.argtypes = [P(Geometry), _c_int, _vp, _c_int, _c_dbl, _vp, _vp,
+                                           _c_int]
     lib.ccpi_plan_create.argtypes = [P(Geometry), P(_vp)]
     lib.ccpi_plan_autotune.argtypes = [_vp, _vp, _i32p]
     lib.ccpi_plan_set_cone_backprojector.argtypes = [_vp, _c_int]

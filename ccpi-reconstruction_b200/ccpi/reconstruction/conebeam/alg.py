@@ -175,14 +175,17 @@ def create_sinogram(source_x, source_y, source_z, detector_x, h_pixels, v_pixels
 
 def reconstruct_explicit(algorithm, source, detector_x, h_pixels, v_pixels, angles, sino,
                          grid_offset, voxel_size, shape, niterations, regularize=0.0,
-                         norm_r=None):
+                         norm_r=None, backprojector="gather"):
     """A cone-beam solver on an explicit geometry with host arrays
     (``ccpi_reconstruct``; the reference's reconstruction_alg::reconstruct
     on an explicitly set instrument, Core/src/algorithms.hpp:13-20).
     algorithm: "cgls", "sirt", "mlem", "cgls_tikhonov" or "cgls_TVreg";
     angles in radians; sino (n_angles, n_h, n_v) log data; returns the
     clamped volume of `shape`; norm_r (optional, one entry per iteration)
-    receives |A^T r| for the CGLS family."""
+    receives |A^T r| for the CGLS family.  backprojector: "gather" (the
+    default, deterministic: b2D bit for bit) or "scatter" (the CGLS family
+    back-projects with the ray-driven scatter, ``CCPI_RECON_CONE_SCATTER``:
+    faster, equal to float rounding)."""
     algs = {"cgls": N.CGLS, "sirt": N.SIRT, "mlem": N.MLEM, "cgls_tikhonov": N.CGLS_TIKHONOV,
             "cgls_TVreg": N.CGLS_TV}
     if algorithm not in algs:
@@ -203,9 +206,13 @@ def reconstruct_explicit(algorithm, source, detector_x, h_pixels, v_pixels, angl
     g.nx, g.ny, g.nz = (int(x) for x in shape)
     out = np.zeros(tuple(int(x) for x in shape), np.float32)
     norms = np.zeros(max(int(niterations), 1), np.float64)
-    N.check(N.lib.ccpi_reconstruct(ctypes.byref(g), algs[algorithm], s.ctypes.data,
-                                   int(niterations), float(regularize), norms.ctypes.data,
-                                   out.ctypes.data), "reconstruct_explicit")
+    forms = {"gather": 0, "scatter": N.RECON_CONE_SCATTER}
+    if backprojector not in forms:
+        raise ValueError(f"unknown backprojector {backprojector!r}")
+    N.check(N.lib.ccpi_reconstruct_flags(ctypes.byref(g), algs[algorithm], s.ctypes.data,
+                                         int(niterations), float(regularize),
+                                         norms.ctypes.data, out.ctypes.data,
+                                         forms[backprojector]), "reconstruct_explicit")
     if norm_r is not None:
         nr = np.asarray(norm_r)
         n = min(int(niterations), nr.shape[0])

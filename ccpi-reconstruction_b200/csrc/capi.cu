@@ -795,6 +795,11 @@ int ccpi_cb_create_sinogram(const ccpi_geometry *geometry, const float *volume, 
 
 int ccpi_reconstruct(const ccpi_geometry *geometry, int alg, const float *sino, int niter,
                      double regularize, double *norms, float *volume) {
+  return ccpi_reconstruct_flags(geometry, alg, sino, niter, regularize, norms, volume, 0);
+}
+
+int ccpi_reconstruct_flags(const ccpi_geometry *geometry, int alg, const float *sino, int niter,
+                           double regularize, double *norms, float *volume, int flags) {
   ccpi::g_last_error.clear();
   if (!geometry || !sino || !volume) {
     set_error("ccpi_reconstruct: need a geometry and host buffers");
@@ -804,9 +809,16 @@ int ccpi_reconstruct(const ccpi_geometry *geometry, int alg, const float *sino, 
     set_error("ccpi_reconstruct: unknown algorithm or negative iteration count");
     return 1;
   }
+  if (flags & ~CCPI_RECON_CONE_SCATTER) {
+    set_error("ccpi_reconstruct_flags: unknown flag bits");
+    return 1;
+  }
   PlanHolder P;
   if (ccpi::plan_create(geometry, &P.p))
     return 2;
+  if ((flags & CCPI_RECON_CONE_SCATTER) && geometry->kind == CCPI_CONE &&
+      ccpi::set_cone_backprojector(P.p, 1))
+    return 1;
   const i64 V = P.p->nvox, Pn = P.p->npix;
   DevBuf dsino, dx;
   if (!dsino.alloc(Pn * 4) || !dx.alloc(V * 4))

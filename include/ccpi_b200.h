@@ -229,6 +229,22 @@ int ccpi_cb_create_sinogram(const ccpi_geometry *geometry,
 int ccpi_reconstruct(const ccpi_geometry *geometry, int alg, const float *sino, int niter,
                      double regularize, double *norms, float *volume);
 
+/* Flags of ccpi_reconstruct_flags. */
+enum {
+  CCPI_RECON_CONE_SCATTER = 1 /* cone beam: the CGLS family back-projects with
+                                 the ray-driven scatter
+                                 (ccpi_plan_set_cone_backprojector 1): faster,
+                                 equal to the gather to float rounding, the
+                                 order of its additions not fixed; SIRT and
+                                 MLEM are unchanged */
+};
+
+/* ccpi_reconstruct with flags (0 gives ccpi_reconstruct).  No reference
+ * counterpart beyond ccpi_reconstruct's: the flags choose among this
+ * build's equivalent forms.  Unknown flag bits are an error. */
+int ccpi_reconstruct_flags(const ccpi_geometry *geometry, int alg, const float *sino, int niter,
+                           double regularize, double *norms, float *volume, int flags);
+
 /* ---------------------------------------------------------------------
  * Device-level calls (device buffers; asynchronous on `stream` unless
  * stated).  Replace the core projector and solver entry points the

@@ -152,6 +152,34 @@ def test_cone_cgls_norms_vs_fp64(cuda):
     assert np.all(nz == 0)
 
 
+@pytest.mark.parametrize("algorithm", ["cgls", "sirt"])
+def test_reconstruct_explicit_scatter_flag(algorithm, cuda):
+    """ccpi_reconstruct_flags with CCPI_RECON_CONE_SCATTER: CGLS back-projects
+    with the ray-driven scatter and agrees with the default (gather) solve to
+    1e-5 rel-L2 after 4 iterations; SIRT always uses the gather and is
+    unchanged bit for bit; unknown flag bits are an error."""
+    import ctypes
+
+    from ccpi.reconstruction import _native as N
+    from ccpi.reconstruction.conebeam import alg as A
+    g, s = C.cone_case()
+    args = (algorithm, g.source, g.detector_x, g.h_pixels, g.v_pixels, g.angles, s, g.origin,
+            g.size, g.shape, 4)
+    base = A.reconstruct_explicit(*args)
+    fast = A.reconstruct_explicit(*args, backprojector="scatter")
+    if algorithm == "sirt":
+        assert np.array_equal(fast, base)
+    else:
+        assert rel_l2(fast, base) <= 1e-5
+    with pytest.raises(ValueError):
+        A.reconstruct_explicit(*args, backprojector="bogus")
+    geo = N.Geometry()
+    out = np.zeros(3, np.float32)
+    assert N.lib.ccpi_reconstruct_flags(ctypes.byref(geo), 0, out.ctypes.data, 1, 0.0, None,
+                                        out.ctypes.data, 2) == 1
+    assert b"unknown flag" in N.lib.ccpi_last_error()
+
+
 @pytest.mark.parametrize("algorithm,alg,lam", [("cgls", 0, 0.0), ("sirt", 1, 0.0),
                                                ("cgls_TVreg", 4, 0.01)])
 def test_reconstruct_explicit_equals_device_solve(algorithm, alg, lam, cuda):
