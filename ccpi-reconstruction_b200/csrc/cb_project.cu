@@ -22,6 +22,7 @@
 // shared-memory accumulator with float atomics (unspecified order, equal to
 // the reference to float rounding).
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -537,8 +538,8 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
         float *col = vol + i64(cell) * nz;
         int ck = -1, ckn = -1, ckey = -1; // the lane's current run
         float r1 = 0.0f, r2 = 0.0f;
-#pragma unroll
-        for (int j = 0; j < RPL; j++) {
+        auto step = [&](int j, auto tag) {
+          constexpr bool INBAND = decltype(tag)::value;
           const int v = vb + lane * RPL + j;
           // the back projector's rule for this row (c2D.cpp:680-750): a
           // band row feeds its slice k and the neighbour on the source's
@@ -547,8 +548,8 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
           int k = -1, kn = -1;
           bool up = false;
           float w1 = 0.0f, w2 = 0.0f;
-          if (vok[j]) {
-            if (v >= band.x && v < band.y) {
+          if (INBAND || vok[j]) {
+            if (INBAND || (v >= band.x && v < band.y)) {
               const int kk = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[j])));
               const int kkn = below[j] ? kk - 1 : kk + 1;
               if (unsigned(kk) <= unsigned(nzm1) && unsigned(kkn) <= unsigned(nzm1)) {
@@ -604,6 +605,17 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
             r1 = __fadd_rn(r1, __fmul_rn(p[j], w1));
             r2 = __fadd_rn(r2, __fmul_rn(p[j], w2));
           }
+        };
+        // every row of the pass valid and inside the column's band: only
+        // the band rule runs (the test is the same for the whole warp)
+        if (vb + 32 * RPL <= band.y && vb >= band.x && vb + 32 * RPL <= g.nv) {
+#pragma unroll
+          for (int j = 0; j < RPL; j++)
+            step(j, std::true_type{});
+        } else {
+#pragma unroll
+          for (int j = 0; j < RPL; j++)
+            step(j, std::false_type{});
         }
         if (ck >= 0) {
           atomicAdd(col + ck, r1);
