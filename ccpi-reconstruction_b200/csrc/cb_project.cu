@@ -22,7 +22,6 @@
 // shared-memory accumulator with float atomics (unspecified order, equal to
 // the reference to float rounding).
 #include <algorithm>
-#include <type_traits>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -538,58 +537,12 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
         float *col = vol + i64(cell) * nz;
         int ck = -1, ckn = -1, ckey = -1; // the lane's current run
         float r1 = 0.0f, r2 = 0.0f;
-        auto step = [&](int j, auto tag) {
-          constexpr bool INBAND = decltype(tag)::value;
-          const int v = vb + lane * RPL + j;
-          // the back projector's rule for this row (c2D.cpp:680-750): a
-          // band row feeds its slice k and the neighbour on the source's
-          // side (k - 1 below the source, k + 1 above), a row below the
-          // band k and k - 1, a row above it k and k + 1
-          int k = -1, kn = -1;
-          bool up = false;
-          float w1 = 0.0f, w2 = 0.0f;
-          if (INBAND || vok[j]) {
-            if (INBAND || (v >= band.x && v < band.y)) {
-              const int kk = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[j])));
-              const int kkn = below[j] ? kk - 1 : kk + 1;
-              if (unsigned(kk) <= unsigned(nzm1) && unsigned(kkn) <= unsigned(nzm1)) {
-                const float mz = fmin_ref(__fmul_rn(svz[below[j] ? kk : kk + 1], izv[j]), a1);
-                k = kk;
-                kn = kkn;
-                up = !below[j];
-                w1 = __fsub_rn(mz, a0);
-                w2 = __fsub_rn(a1, mz);
-              }
-            } else if (v < band.x) {
-              const int kk = int(__fadd_rn(pzbz1, __fmul_rn(av, dzv[j]))) - 1;
-              if (kk > 0 && kk <= nzm1) {
-                const float mz = fmin_ref(__fmul_rn(svz[kk], izv[j]), a1);
-                k = kk;
-                kn = kk - 1;
-                w1 = __fsub_rn(mz, a0);
-                w2 = __fsub_rn(a1, mz);
-              } else if (kk == 0) {
-                k = 0;
-                w1 = __fsub_rn(fmin_ref(__fmul_rn(svz[0], izv[j]), a1), a0);
-              }
-            } else {
-              const int kk = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[j])));
-              up = true;
-              if (kk < nzm1 && kk >= 0) {
-                const float mz = fmin_ref(__fmul_rn(svz[kk + 1], izv[j]), a1);
-                k = kk;
-                kn = kk + 1;
-                w1 = __fsub_rn(mz, a0);
-                w2 = __fsub_rn(a1, mz);
-              } else if (kk == nzm1) {
-                k = nzm1;
-                w1 = __fsub_rn(fmin_ref(__fmul_rn(svz[nz], izv[j]), a1), a0);
-              }
-            }
-          }
+        // one row's run logic: a run of rows with the same slice and side
+        // sums its two products in registers; when the slice changes the
+        // run's two sums go to its slice and neighbour
+        auto run = [&](int k, int kn, bool up, float s1, float s2) {
           const int key = k >= 0 ? 2 * k + (up ? 1 : 0) : -1;
           if (key != ckey) {
-            // the run ends: its two sums go to its slice and neighbour
             if (ck >= 0) {
               atomicAdd(col + ck, r1);
               if (ckn >= 0)
@@ -602,20 +555,95 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
             r2 = 0.0f;
           }
           if (k >= 0) {
-            r1 = __fadd_rn(r1, __fmul_rn(p[j], w1));
-            r2 = __fadd_rn(r2, __fmul_rn(p[j], w2));
+            r1 = __fadd_rn(r1, s1);
+            r2 = __fadd_rn(r2, s2);
           }
         };
-        // every row of the pass valid and inside the column's band: only
-        // the band rule runs (the test is the same for the whole warp)
         if (vb + 32 * RPL <= band.y && vb >= band.x && vb + 32 * RPL <= g.nv) {
+          // every row of the pass valid and inside the column's band (the
+          // test is the same for the whole warp): the band rule alone, rows
+          // j and j + 1 as packed pairs with the same unfused operations
+          // per row (a packed product only feeds scalar adds)
 #pragma unroll
-          for (int j = 0; j < RPL; j++)
-            step(j, std::true_type{});
+          for (int j = 0; j + 1 < RPL; j += 2) {
+            const float2 kz = mul2_rn(make_float2(av, av), make_float2(dzv[j], dzv[j + 1]));
+            const int k0 = int(__fadd_rn(pzbz, kz.x)), k1 = int(__fadd_rn(pzbz, kz.y));
+            const int n0 = below[j] ? k0 - 1 : k0 + 1, n1 = below[j + 1] ? k1 - 1 : k1 + 1;
+            const bool ok0 = unsigned(k0) <= unsigned(nzm1) && unsigned(n0) <= unsigned(nzm1);
+            const bool ok1 = unsigned(k1) <= unsigned(nzm1) && unsigned(n1) <= unsigned(nzm1);
+            const float z0 = ok0 ? svz[below[j] ? k0 : k0 + 1] : 0.0f;
+            const float z1 = ok1 ? svz[below[j + 1] ? k1 : k1 + 1] : 0.0f;
+            const float2 pl = mul2_rn(make_float2(z0, z1), make_float2(izv[j], izv[j + 1]));
+            const float2 mz = make_float2(fmin_ref(pl.x, a1), fmin_ref(pl.y, a1));
+            const float2 w1 = sub2_rn(mz, make_float2(a0, a0));
+            const float2 w2 = sub2_rn(make_float2(a1, a1), mz);
+            const float2 pp = make_float2(p[j], p[j + 1]);
+            const float2 s1 = mul2_rn(pp, w1), s2 = mul2_rn(pp, w2);
+            run(ok0 ? k0 : -1, ok0 ? n0 : -1, !below[j], s1.x, s2.x);
+            run(ok1 ? k1 : -1, ok1 ? n1 : -1, !below[j + 1], s1.y, s2.y);
+          }
+          if (RPL % 2) {
+            constexpr int j = RPL - 1; // the odd row, alone
+            const int k0 = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[j])));
+            const int n0 = below[j] ? k0 - 1 : k0 + 1;
+            const bool ok0 = unsigned(k0) <= unsigned(nzm1) && unsigned(n0) <= unsigned(nzm1);
+            const float z0 = ok0 ? svz[below[j] ? k0 : k0 + 1] : 0.0f;
+            const float mz = fmin_ref(__fmul_rn(z0, izv[j]), a1);
+            run(ok0 ? k0 : -1, ok0 ? n0 : -1, !below[j], __fmul_rn(p[j], __fsub_rn(mz, a0)),
+                __fmul_rn(p[j], __fsub_rn(a1, mz)));
+          }
         } else {
 #pragma unroll
-          for (int j = 0; j < RPL; j++)
-            step(j, std::false_type{});
+          for (int j = 0; j < RPL; j++) {
+            const int v = vb + lane * RPL + j;
+            // the back projector's rule for this row (c2D.cpp:680-750): a
+            // band row feeds its slice k and the neighbour on the source's
+            // side (k - 1 below the source, k + 1 above), a row below the
+            // band k and k - 1, a row above it k and k + 1
+            int k = -1, kn = -1;
+            bool up = false;
+            float w1 = 0.0f, w2 = 0.0f;
+            if (vok[j]) {
+              if (v >= band.x && v < band.y) {
+                const int kk = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[j])));
+                const int kkn = below[j] ? kk - 1 : kk + 1;
+                if (unsigned(kk) <= unsigned(nzm1) && unsigned(kkn) <= unsigned(nzm1)) {
+                  const float mz = fmin_ref(__fmul_rn(svz[below[j] ? kk : kk + 1], izv[j]), a1);
+                  k = kk;
+                  kn = kkn;
+                  up = !below[j];
+                  w1 = __fsub_rn(mz, a0);
+                  w2 = __fsub_rn(a1, mz);
+                }
+              } else if (v < band.x) {
+                const int kk = int(__fadd_rn(pzbz1, __fmul_rn(av, dzv[j]))) - 1;
+                if (kk > 0 && kk <= nzm1) {
+                  const float mz = fmin_ref(__fmul_rn(svz[kk], izv[j]), a1);
+                  k = kk;
+                  kn = kk - 1;
+                  w1 = __fsub_rn(mz, a0);
+                  w2 = __fsub_rn(a1, mz);
+                } else if (kk == 0) {
+                  k = 0;
+                  w1 = __fsub_rn(fmin_ref(__fmul_rn(svz[0], izv[j]), a1), a0);
+                }
+              } else {
+                const int kk = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[j])));
+                up = true;
+                if (kk < nzm1 && kk >= 0) {
+                  const float mz = fmin_ref(__fmul_rn(svz[kk + 1], izv[j]), a1);
+                  k = kk;
+                  kn = kk + 1;
+                  w1 = __fsub_rn(mz, a0);
+                  w2 = __fsub_rn(a1, mz);
+                } else if (kk == nzm1) {
+                  k = nzm1;
+                  w1 = __fsub_rn(fmin_ref(__fmul_rn(svz[nz], izv[j]), a1), a0);
+                }
+              }
+            }
+            run(k, kn, up, __fmul_rn(p[j], w1), __fmul_rn(p[j], w2));
+          }
         }
         if (ck >= 0) {
           atomicAdd(col + ck, r1);

@@ -114,6 +114,11 @@ def test_cone_tall_columns_atomic_path(cuda):
     ok = np.isfinite(b_ref)
     assert np.array_equal(np.isfinite(b_gpu), ok)
     assert max_rel(b_gpu[ok], b_ref[ok]) <= TOL
+    # the ray-driven scatter has no column-height limit
+    p.set_cone_backprojector(1)
+    b_sc = run(p, "backward", pix, cuda)
+    assert np.array_equal(np.isfinite(b_sc), ok)
+    assert max_rel(b_sc[ok], b_ref[ok]) <= TOL
 
 
 @pytest.mark.parametrize("kind", ["parallel", "cone"])
