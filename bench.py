@@ -942,6 +942,7 @@ def run_autograd(args):
     torch.cuda.set_device(dev)
     n, na, nd, nb = 256, 360, 384, 8
     plan = cone_plan(n, 2.0, na, nd, 1.6, 500.0, 500.0)
+    bp_kernel, t_tune = pick_cone_bp(plan, args.cone_bp)
     A = Projector(plan)
     xt = torch.stack([ellipsoids(torch, dev, n, 40, (5.0, 60.0), seed=50 + b) for b in range(nb)])
     with torch.no_grad():
@@ -983,7 +984,11 @@ def run_autograd(args):
         fp_ms=1000 * t_fp, bp_ms=1000 * t_bp,
         projector_rays_per_s={"forward": P / t_fp, "backward": P / t_bp},
         loss_first=l0, loss_after=l1, dot_test_rel=abs(lhs - rhs) / abs(lhs),
-        gpu_launches=2 * nb * args.steps, clocks=clk)))
+        back_projector={"kernel": bp_kernel, "choice": args.cone_bp, "autotune_seconds": t_tune},
+        # per step: one batched forward launch; the batched back projection
+        # is one gather launch, or one scatter launch per volume
+        gpu_launches=(1 + (nb if bp_kernel == "cb_bp_scatter" else 1)) * args.steps,
+        clocks=clk)))
 
 
 def run_cone_projectors(args):

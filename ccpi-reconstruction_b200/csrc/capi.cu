@@ -920,7 +920,9 @@ static int project_batch(const char *what, const ccpi_plan *plan, int n, const f
   }
   const cudaStream_t st = cudaStream_t(stream);
   ccpi::Epi e{};
-  if (plan->g.kind == CCPI_CONE && n > 0) {
+  // cone: one launch for the batch, except back projection on a plan set to
+  // the ray-driven scatter, which runs the scatter item by item
+  if (plan->g.kind == CCPI_CONE && n > 0 && (fwd || !plan->g.tune_scatter)) {
     const int rc = fwd ? ccpi::cb_forward(plan->g, in, out, ccpi::EPI_STORE, e, plan->hrange,
                                           plan->fp_grid, st, n)
                        : ccpi::cb_backward(plan->g, in, out, ccpi::EPI_STORE, e, plan->err, st, n);

@@ -308,9 +308,9 @@ int ccpi_backward(const ccpi_plan *plan, const float *d_sino, float *d_volume,
  * direction, the batch sharing each ray's xy walk and each column's ray
  * list (f2D / b2D, Core/src/c2D.cpp:469-625, :948-1119, called once per
  * item in the reference); parallel beam one launch per item.  The cone
- * batch back projection is the voxel gather whichever form
- * ccpi_plan_set_cone_backprojector chose for single calls.  Every item
- * must start on a 16-byte boundary. */
+ * batch back projection is one gather launch on a gather plan; on a plan
+ * set to the scatter (ccpi_plan_set_cone_backprojector 1) it runs the
+ * scatter item by item.  Every item must start on a 16-byte boundary. */
 int ccpi_forward_batch(const ccpi_plan *plan, int n, const float *d_volumes, float *d_sinos,
                        void *stream);
 int ccpi_backward_batch(const ccpi_plan *plan, int n, const float *d_sinos, float *d_volumes,

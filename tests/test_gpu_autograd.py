@@ -149,3 +149,11 @@ def test_batch_projection_equals_per_item(kind, cuda):
             assert torch.equal(by[b], p.backward(y[b])), b
         else:
             assert max_rel(by[b].cpu().numpy(), p.backward(y[b]).cpu().numpy()) <= 1e-5
+    if kind.startswith("cone"):
+        # a plan set to the scatter back-projects a batch item by item with
+        # it: equal to the gather's batch within the projector tolerance
+        p.set_cone_backprojector(1)
+        bs = torch.empty_like(by)
+        p.backward_batch(y, bs)
+        for b in range(n):
+            assert max_rel(bs[b].cpu().numpy(), by[b].cpu().numpy()) <= 1e-5, b
