@@ -579,22 +579,17 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
             const float2 w2 = sub2_rn(make_float2(a1, a1), mz);
             const float2 pp = make_float2(p[j], p[j + 1]);
             const float2 s1 = mul2_rn(pp, w1), s2 = mul2_rn(pp, w2);
-            if (RPL == 2) {
-              // a lane's two rows are its whole pass: one run (the same
-              // slice and side) adds the two rows' sums, two runs add each
-              // row's, with no run state
-              const bool same = ok0 && ok1 && k0 == k1 && below[j] == below[j + 1];
-              if (ok0) {
-                atomicAdd(col + k0, same ? __fadd_rn(s1.x, s1.y) : s1.x);
-                atomicAdd(col + n0, same ? __fadd_rn(s2.x, s2.y) : s2.x);
-              }
-              if (ok1 && !same) {
-                atomicAdd(col + k1, s1.y);
-                atomicAdd(col + n1, s2.y);
-              }
-            } else {
-              run(ok0 ? k0 : -1, ok0 ? n0 : -1, !below[j], s1.x, s2.x);
-              run(ok1 ? k1 : -1, ok1 ? n1 : -1, !below[j + 1], s1.y, s2.y);
+            // the pair's runs, with no run state: one pair of atomics when
+            // both rows share slice and side (their sums added in row
+            // order), else one pair per row
+            const bool same = ok0 && ok1 && k0 == k1 && below[j] == below[j + 1];
+            if (ok0) {
+              atomicAdd(col + k0, same ? __fadd_rn(s1.x, s1.y) : s1.x);
+              atomicAdd(col + n0, same ? __fadd_rn(s2.x, s2.y) : s2.x);
+            }
+            if (ok1 && !same) {
+              atomicAdd(col + k1, s1.y);
+              atomicAdd(col + n1, s2.y);
             }
           }
           if (RPL % 2) {
@@ -604,8 +599,10 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
             const bool ok0 = unsigned(k0) <= unsigned(nzm1) && unsigned(n0) <= unsigned(nzm1);
             const float z0 = ok0 ? svz[below[j] ? k0 : k0 + 1] : 0.0f;
             const float mz = fmin_ref(__fmul_rn(z0, izv[j]), a1);
-            run(ok0 ? k0 : -1, ok0 ? n0 : -1, !below[j], __fmul_rn(p[j], __fsub_rn(mz, a0)),
-                __fmul_rn(p[j], __fsub_rn(a1, mz)));
+            if (ok0) {
+              atomicAdd(col + k0, __fmul_rn(p[j], __fsub_rn(mz, a0)));
+              atomicAdd(col + n0, __fmul_rn(p[j], __fsub_rn(a1, mz)));
+            }
           }
         } else {
 #pragma unroll
