@@ -513,11 +513,18 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
     for (int vb = 0; n >= 2 && vb < g.nv; vb += 32 * RPL) {
       float p[RPL], dzv[RPL], izv[RPL];
       bool vok[RPL], below[RPL];
+      // per row, fixed by its side of the source: the neighbour's step, the
+      // slice plane the weights use (k or k + 1) and the lowest slice whose
+      // neighbour stays inside the column
+      int dk[RPL], off[RPL], klo[RPL];
 #pragma unroll
       for (int j = 0; j < RPL; j++) {
         const int v = vb + lane * RPL + j;
         vok[j] = v < g.nv;
         below[j] = v < mid;
+        dk[j] = below[j] ? -1 : 1;
+        off[j] = below[j] ? 0 : 1;
+        klo[j] = below[j] ? 1 : 0;
         dzv[j] = vok[j] ? g.dz[v] : 0.0f;
         izv[j] = vok[j] ? g.iz[v] : 0.0f;
         const float y = vok[j] ? __ldg(pix + rbase + v) : 0.0f;
@@ -568,11 +575,12 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
           for (int j = 0; j + 1 < RPL; j += 2) {
             const float2 kz = mul2_rn(make_float2(av, av), make_float2(dzv[j], dzv[j + 1]));
             const int k0 = int(__fadd_rn(pzbz, kz.x)), k1 = int(__fadd_rn(pzbz, kz.y));
-            const int n0 = below[j] ? k0 - 1 : k0 + 1, n1 = below[j + 1] ? k1 - 1 : k1 + 1;
-            const bool ok0 = unsigned(k0) <= unsigned(nzm1) && unsigned(n0) <= unsigned(nzm1);
-            const bool ok1 = unsigned(k1) <= unsigned(nzm1) && unsigned(n1) <= unsigned(nzm1);
-            const float z0 = ok0 ? svz[below[j] ? k0 : k0 + 1] : 0.0f;
-            const float z1 = ok1 ? svz[below[j + 1] ? k1 : k1 + 1] : 0.0f;
+            // k and its neighbour k -/+ 1 inside [0, nz - 1]: one range test
+            // (a one-slice column holds no neighbour)
+            const bool ok0 = nzm1 > 0 && unsigned(k0 - klo[j]) <= unsigned(nzm1 - 1);
+            const bool ok1 = nzm1 > 0 && unsigned(k1 - klo[j + 1]) <= unsigned(nzm1 - 1);
+            const float z0 = ok0 ? svz[k0 + off[j]] : 0.0f;
+            const float z1 = ok1 ? svz[k1 + off[j + 1]] : 0.0f;
             const float2 pl = mul2_rn(make_float2(z0, z1), make_float2(izv[j], izv[j + 1]));
             const float2 mz = make_float2(fmin_ref(pl.x, a1), fmin_ref(pl.y, a1));
             const float2 w1 = sub2_rn(mz, make_float2(a0, a0));
@@ -582,26 +590,27 @@ __global__ void __launch_bounds__(kFpWarps * 32, 8)
             // the pair's runs, with no run state: one pair of atomics when
             // both rows share slice and side (their sums added in row
             // order), else one pair per row
-            const bool same = ok0 && ok1 && k0 == k1 && below[j] == below[j + 1];
+            const bool same = ok0 && ok1 && k0 == k1 && dk[j] == dk[j + 1];
             if (ok0) {
-              atomicAdd(col + k0, same ? __fadd_rn(s1.x, s1.y) : s1.x);
-              atomicAdd(col + n0, same ? __fadd_rn(s2.x, s2.y) : s2.x);
+              float *c0 = col + k0;
+              atomicAdd(c0, same ? __fadd_rn(s1.x, s1.y) : s1.x);
+              atomicAdd(c0 + dk[j], same ? __fadd_rn(s2.x, s2.y) : s2.x);
             }
             if (ok1 && !same) {
-              atomicAdd(col + k1, s1.y);
-              atomicAdd(col + n1, s2.y);
+              float *c1 = col + k1;
+              atomicAdd(c1, s1.y);
+              atomicAdd(c1 + dk[j + 1], s2.y);
             }
           }
           if (RPL % 2) {
             constexpr int j = RPL - 1; // the odd row, alone
             const int k0 = int(__fadd_rn(pzbz, __fmul_rn(av, dzv[j])));
-            const int n0 = below[j] ? k0 - 1 : k0 + 1;
-            const bool ok0 = unsigned(k0) <= unsigned(nzm1) && unsigned(n0) <= unsigned(nzm1);
-            const float z0 = ok0 ? svz[below[j] ? k0 : k0 + 1] : 0.0f;
+            const bool ok0 = nzm1 > 0 && unsigned(k0 - klo[j]) <= unsigned(nzm1 - 1);
+            const float z0 = ok0 ? svz[k0 + off[j]] : 0.0f;
             const float mz = fmin_ref(__fmul_rn(z0, izv[j]), a1);
             if (ok0) {
               atomicAdd(col + k0, __fmul_rn(p[j], __fsub_rn(mz, a0)));
-              atomicAdd(col + n0, __fmul_rn(p[j], __fsub_rn(a1, mz)));
+              atomicAdd(col + k0 + dk[j], __fmul_rn(p[j], __fsub_rn(a1, mz)));
             }
           }
         } else {
